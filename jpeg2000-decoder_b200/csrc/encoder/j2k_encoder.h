@@ -1,0 +1,68 @@
+/*
+ * j2k_encoder.h — minimal JPEG 2000 Part-1 (ITU-T T.800) codestream writer.
+ *
+ * The reference library ships an empty encoder shell (decoder/core/src/encoderconcrete.cpp),
+ * so every codestream the tests and the benchmark decode is produced here from seeded
+ * synthetic images.  Supported: reversible 5/3 + RCT, irreversible 9/7 + ICT with
+ * scalar-expounded quantisation, rectangular tiles anchored at the origin, 32/64 code-blocks,
+ * quality layers chosen by slope thresholds, LRCP/RLCP/RPCL/PCRL/CPRL progression with one
+ * precinct per resolution, and the BYPASS / RESET / TERMALL / SEGSYM mode switches.
+ *
+ * The irreversible path writes one guard bit by default: the reference's Tier-1 places the
+ * most significant magnitude bit at (expn - 1 - missing) (decoder/codec/src/
+ * bmi_block_decoder.cpp:708-710), which is only the T.800 position when G == 1.
+ */
+#ifndef J2K_ENCODER_H
+#define J2K_ENCODER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum j2kenc_progression { J2KENC_LRCP = 0, J2KENC_RLCP = 1, J2KENC_RPCL = 2, J2KENC_PCRL = 3, J2KENC_CPRL = 4 };
+
+/* code-block style bits, as written in the COD marker (T.800 Table A.19) */
+enum j2kenc_mode {
+  J2KENC_BYPASS = 0x01,
+  J2KENC_RESET = 0x02,
+  J2KENC_TERMALL = 0x04,
+  J2KENC_CAUSAL = 0x08, /* not supported by this writer */
+  J2KENC_PTERM = 0x10,  /* accepted, termination is the plain T.800 flush */
+  J2KENC_SEGSYM = 0x20
+};
+
+typedef struct j2kenc_params {
+  int reversible;     /* 1: 5/3 integer + RCT; 0: 9/7 + ICT */
+  int levels;         /* decomposition levels, 0..10 */
+  int cbw_exp;        /* log2 code-block width  (2..10, cbw_exp + cbh_exp <= 12) */
+  int cbh_exp;        /* log2 code-block height */
+  int tile_w;         /* 0: one tile covering the image */
+  int tile_h;
+  int num_layers;     /* 1..32 */
+  double layer_bpp[32]; /* cumulative target bits per pixel for each layer; <= 0: all passes */
+  int progression;    /* j2kenc_progression */
+  int mode;           /* OR of j2kenc_mode */
+  int use_mct;        /* apply RCT/ICT when there are >= 3 components */
+  int guard_bits;     /* 0: 1 for 9/7, 2 for 5/3 */
+  double base_step;   /* 9/7: quantiser step for a unit-energy band, in sample units */
+  int num_threads;    /* 0: hardware concurrency */
+} j2kenc_params;
+
+void j2kenc_default_params(j2kenc_params *p);
+
+/*
+ * Encode an image of `ncomp` planes (plane-major, row-major, `bitdepth`-bit unsigned samples
+ * in uint16) into a raw J2K codestream.  *out is allocated with malloc; free it with
+ * j2kenc_free.  Returns 0 on success, a negative value on a parameter error.
+ */
+int j2kenc_encode(const uint16_t *planes, int width, int height, int ncomp, int bitdepth,
+                  const j2kenc_params *params, uint8_t **out, size_t *out_len);
+void j2kenc_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
