@@ -1,0 +1,86 @@
+/*
+ * codestream.h — host-side JPEG 2000 Part-1 front end: marker segments, tiles and
+ * Tier-2 packet headers, producing a decode plan (plan.h) for the device.
+ *
+ * Mirrors the role of the reference's codestream layer, which stays on the host there too:
+ * dec_syntax.cpp (SIZ/COD/COC/QCD/QCC/RGN/COM parsing, :134-421), dec_packet.cpp (packet
+ * headers, pass counts, Lblock, lengths, :66-221; progression orders :384-730),
+ * dec_tagtree.cpp (tag trees), dec_init.cpp (tile / subband / code-block geometry,
+ * :645-1056) and dec_jp2.cpp (JP2 wrapper, BMI_dec_info sizes, :420-597).
+ */
+#ifndef J2K_CODESTREAM_H
+#define J2K_CODESTREAM_H
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+
+namespace j2k {
+
+enum ParseStatus {
+  PARSE_OK = 0,
+  PARSE_ERR_TRUNCATED = -1,
+  PARSE_ERR_MARKER = -2,
+  PARSE_ERR_UNSUPPORTED = -3,
+  PARSE_ERR_INVALID = -4,
+  PARSE_ERR_PACKET = -5
+};
+
+struct DecodeOptions {
+  int discard_levels = 0;    /* decode at 1/2^n resolution (reference mDwtDecodeTopLevel) */
+  int max_layers = 0;        /* 0: all layers */
+  unsigned ignore_components = 0; /* bit c set: component c is not decoded */
+};
+
+/* Header-level description (main header only; no Tier-2). */
+struct StreamHeader {
+  int width = 0, height = 0, x0 = 0, y0 = 0;
+  int tile_w = 0, tile_h = 0, tx0 = 0, ty0 = 0;
+  int ncomp = 0;
+  int depth[J2K_MAX_COMPONENTS] = {0};
+  int is_signed[J2K_MAX_COMPONENTS] = {0};
+  int sub_x[J2K_MAX_COMPONENTS] = {0}, sub_y[J2K_MAX_COMPONENTS] = {0};
+  int progression = 0, layers = 0, mct = 0;
+  int levels[J2K_MAX_COMPONENTS] = {0};
+  int cbw_exp[J2K_MAX_COMPONENTS] = {0}, cbh_exp[J2K_MAX_COMPONENTS] = {0};
+  int cbstyle[J2K_MAX_COMPONENTS] = {0};
+  int reversible[J2K_MAX_COMPONENTS] = {0};
+  int ppx[J2K_MAX_COMPONENTS][J2K_MAX_LEVELS + 1] = {{0}}, ppy[J2K_MAX_COMPONENTS][J2K_MAX_LEVELS + 1] = {{0}};
+  int sop = 0, eph = 0;
+  int qstyle[J2K_MAX_COMPONENTS] = {0};
+  int guard[J2K_MAX_COMPONENTS] = {0};
+  uint16_t steps[J2K_MAX_COMPONENTS][3 * J2K_MAX_LEVELS + 1] = {{0}};  /* raw SPqcd/SPqcc values */
+  int roi_shift[J2K_MAX_COMPONENTS] = {0};
+  size_t header_len = 0;    /* bytes up to the first SOT */
+  size_t cs_offset = 0;     /* offset of SOC inside the input (JP2 wrapper) */
+  int ntx() const { return (width - tx0 + tile_w - 1) / tile_w; }
+  int nty() const { return (height - ty0 + tile_h - 1) / tile_h; }
+};
+
+/* The full host-side plan of one image. */
+struct ImagePlan {
+  StreamHeader hdr;
+  j2k_image_info info{};
+  std::vector<j2k_cblk> cblks;
+  std::vector<uint32_t> seglens;
+  std::vector<uint8_t> bytes;         /* Tier-1 bytes, block after block */
+  std::vector<j2k_tilecomp> tilecomps;
+  int out_w = 0, out_h = 0;           /* output size after discard_levels */
+  int discard = 0;
+};
+
+int parse_header(const uint8_t *data, size_t len, StreamHeader &hdr);
+int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImagePlan &plan);
+const char *status_string(int status);
+
+/* 9/7 band gain of the reference's gain folding, computed with the same float operations. */
+float irrev_band_gain(uint16_t spqcd, int bitdepth, int band, int no_dwt);
+/* Constant applied to the reconstructed LL of a coarser level before the next 9/7 level. */
+float irrev_ll_gain();
+
+}  // namespace j2k
+
+#endif
