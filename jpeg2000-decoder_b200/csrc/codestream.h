@@ -83,4 +83,9 @@ float irrev_ll_gain();
 
 }  // namespace j2k
 
+/* opaque handle of the C ABI (include/j2k_gpu.h) */
+struct j2k_plan {
+  j2k::ImagePlan p;
+};
+
 #endif

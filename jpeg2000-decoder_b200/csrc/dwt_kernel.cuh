@@ -1,0 +1,318 @@
+/*
+ * dwt_kernel.cuh — inverse 5/3 and 9/7 DWT levels and the inverse MCT / DC-shift / pack
+ * stage for sm_100a.
+ *
+ * One CTA reconstructs a 64x64 output tile of one resolution level of one
+ * tile-component: it stages the 72x72 interleaved input window (the four quadrants of the
+ * Mallat layout plus a 4-sample whole-sample-symmetric halo) in shared memory with
+ * coalesced loads, runs the horizontal then the vertical lifting steps there, and writes
+ * the 64x64 result with coalesced stores.  Every level is one read and one write of the
+ * level's samples; all tile-components of a batch at a given level share one launch.
+ *
+ * Arithmetic follows the reference exactly so that results are bit-identical:
+ *   9/7: each lifting update is D = S - c * (L + R) with three separately rounded float
+ *        operations (bmi_cpu_dwt_decoder.cpp:2374-2385, vdwt_analyst_line :4975-4993),
+ *        constants of bmi_cpu_dwt.h:31-41; the reconstructed LL entering a finer level is
+ *        multiplied by K_lo*K_lo (:1599, :1626); band gains are folded in by Tier-1.
+ *   5/3: x[2n] -= (x[2n-1] + x[2n+1] + 2) >> 2, x[2n+1] += (x[2n] + x[2n+2]) >> 1 with
+ *        symmetric ends (:2609-2659, :3311-3534); with J2K_FLAG_REF_COMPAT the last
+ *        column rows are rebuilt the way VDWT_R53_LINES does (:3364-3398).
+ * A whole-sample symmetric input extension is preserved by every lifting step, so
+ * mirroring the input once and lifting across the halo gives the same values as the
+ * reference's per-step mirroring at the region edges.
+ */
+#pragma once
+#include <cstdint>
+
+namespace j2k_dev {
+
+constexpr int DWT_T = 64;          // output tile edge
+constexpr int DWT_H = 4;           // halo
+constexpr int DWT_N = DWT_T + 2 * DWT_H;  // 72
+constexpr int DWT_PITCH = DWT_N + 1;      // odd pitch: conflict-free column access
+
+struct DwtLevel {
+  uint64_t base;     // element offset of the tile-component region (same in every buffer)
+  int32_t stride;    // tile-component width
+  int32_t rw, rh;    // size of the resolution being rebuilt
+  int32_t lw, lh;    // size of its low-pass part (resolution r-1)
+  int8_t ll_src;     // buffer holding the LL quadrant: 0 coefficients, 1 B, 2 C
+  int8_t out_dst;    // buffer receiving the level: 1 B, 2 C
+  int8_t ll_gain;    // 9/7: scale the LL quadrant by K_lo^2 (reconstructed LL)
+  int8_t refcompat;  // 5/3: reference column-end arithmetic
+  int32_t tiles_x;
+};
+
+struct DwtTask {
+  uint32_t level;  // index into the DwtLevel array
+  uint16_t tx, ty;
+};
+
+// Output stage: one tile of one image, up to four components.
+struct OutGroup {
+  uint64_t comp_off[4];  // element offsets of the final component regions
+  int8_t comp_buf[4];    // buffer ids (0 coefficients, 1 B, 2 C), -1 = absent
+  int32_t stride[4];
+  int32_t x0, y0, w, h;  // tile rectangle in the output image
+  uint64_t out_off;      // byte offset of the image in the output buffer
+  int32_t pitch_px;      // output width in pixels
+  int16_t fmt, bitdepth;
+  int8_t rev, mct, ncomp, checkout;  // checkout: reference mCheckOutComponent, -1 = all
+  int32_t tiles_x;
+};
+struct OutTask {
+  uint32_t group;
+  uint16_t tx, ty;
+};
+
+__device__ __forceinline__ int mirror(int p, int n) {
+  if (n == 1) return 0;
+  const int period = 2 * (n - 1);
+  p %= period;
+  if (p < 0) p += period;
+  return p >= n ? period - p : p;
+}
+
+__device__ __forceinline__ float lift97(float s, float c, float l, float r) {
+  return __fsub_rn(s, __fmul_rn(c, __fadd_rn(l, r)));
+}
+
+template <bool REV>
+struct DwtTypes;
+template <>
+struct DwtTypes<true> {
+  typedef int32_t T;
+};
+template <>
+struct DwtTypes<false> {
+  typedef float T;
+};
+
+// Lifting along one direction over the staged tile.  `horizontal` selects rows; positions
+// with both neighbours inside the 72-wide window are updated.
+template <bool REV, bool HORIZ>
+__device__ __forceinline__ void lift_tile(typename DwtTypes<REV>::T *t, int lines_begin, int lines_end) {
+  typedef typename DwtTypes<REV>::T T;
+  const int nl = lines_end - lines_begin;
+  const int half = (DWT_N - 2) / 2;  // 35 updates per parity per line
+  constexpr int NSTEP = REV ? 2 : 4;
+  const float coef[4] = {0.44350685204397f, 0.88291107553093f, -0.05298011857296f, -1.58613434205992f};
+#pragma unroll
+  for (int step = 0; step < NSTEP; ++step) {
+    const int parity = step & 1;  // even, odd, even, odd
+    for (int i = threadIdx.x; i < nl * half; i += blockDim.x) {
+      int line = lines_begin + i / half;
+      int pos = 2 - parity + 2 * (i % half);  // even: 2..70, odd: 1..69 (neighbours in [0, 72))
+      T *c, *l, *r;
+      if (HORIZ) {
+        c = t + line * DWT_PITCH + pos;
+        l = c - 1;
+        r = c + 1;
+      } else {
+        c = t + pos * DWT_PITCH + line;
+        l = c - DWT_PITCH;
+        r = c + DWT_PITCH;
+      }
+      if constexpr (REV) {
+        if (parity == 0) *c = *c - ((*l + *r + 2) >> 2);
+        else *c = *c + ((*l + *r) >> 1);
+      } else {
+        *c = lift97(*c, coef[step], *l, *r);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <bool REV>
+__device__ __forceinline__ typename DwtTypes<REV>::T *dwt_buf(int id, void *a, void *b, void *c) {
+  typedef typename DwtTypes<REV>::T T;
+  return (T *)(id == 0 ? a : (id == 1 ? b : c));
+}
+
+template <bool REV>
+__global__ void __launch_bounds__(256) dwt_level_kernel(const DwtLevel *__restrict__ levels,
+                                                        const DwtTask *__restrict__ tasks, int ntasks, void *bufA,
+                                                        void *bufB, void *bufC, float ll_gain_value) {
+  typedef typename DwtTypes<REV>::T T;
+  __shared__ T tile[DWT_N * DWT_PITCH];
+  __shared__ T keep[2][DWT_T];  // reference-compat inputs of the column end
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const DwtTask tk = tasks[task];
+    const DwtLevel L = levels[tk.level];
+    const int ox = tk.tx * DWT_T, oy = tk.ty * DWT_T;
+    const T *A = dwt_buf<REV>(0, bufA, bufB, bufC) + L.base;
+    const T *LLsrc = dwt_buf<REV>(L.ll_src, bufA, bufB, bufC) + L.base;
+    T *out = dwt_buf<REV>(L.out_dst, bufA, bufB, bufC) + L.base;
+    // ---- stage the interleaved window with a mirrored halo
+    for (int i = threadIdx.x; i < DWT_N * DWT_N; i += blockDim.x) {
+      const int iy = i / DWT_N, ix = i % DWT_N;
+      const int y = mirror(oy - DWT_H + iy, L.rh);
+      const int x = mirror(ox - DWT_H + ix, L.rw);
+      const int sy = (y & 1) ? L.lh + (y >> 1) : (y >> 1);
+      const int sx = (x & 1) ? L.lw + (x >> 1) : (x >> 1);
+      T v;
+      if (!(x & 1) && !(y & 1)) {
+        v = LLsrc[(size_t)sy * L.stride + sx];
+        if (!REV && L.ll_gain) v = (T)__fmul_rn((float)v, ll_gain_value);
+      } else {
+        v = A[(size_t)sy * L.stride + sx];
+      }
+      tile[iy * DWT_PITCH + ix] = v;
+    }
+    __syncthreads();
+    if (L.rw > 1) lift_tile<REV, true>(tile, 0, DWT_N);
+    // reference-compat: keep the horizontally transformed inputs the column end reads
+    const int n = L.rh;
+    const bool fix = REV && L.refcompat && n >= 3 && (oy <= n - 1) && (n - 2 < oy + DWT_T);
+    int rowA = -1, rowB = -1;
+    if (fix) {
+      if (!(n & 1)) {
+        rowA = n - 3;  // H[m-2]
+      } else {
+        const int m = (n + 1) / 2;
+        rowA = n - 3;                    // L[m-2]
+        rowB = (m >= 3) ? n - 4 : 1;     // H[m-3] (H[0] when m == 2)
+      }
+      for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
+        keep[0][c] = tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+        if (rowB >= 0) keep[1][c] = tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+      }
+      __syncthreads();
+    }
+    if (L.rh > 1) lift_tile<REV, false>(tile, DWT_H, DWT_H + DWT_T);
+    if constexpr (REV) {
+      if (fix) {
+      for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
+        T *col = tile + DWT_H + c;
+        const int r1 = n - 1 - oy + DWT_H, r2 = n - 2 - oy + DWT_H, r3 = n - 3 - oy + DWT_H;
+        if (!(n & 1)) {
+          col[r1 * DWT_PITCH] = keep[0][c] + col[r2 * DWT_PITCH];
+        } else {
+          const T hx = keep[1][c];
+          const T x1 = keep[0][c] - ((hx + 1) >> 1);
+          col[r1 * DWT_PITCH] = x1;
+          col[r2 * DWT_PITCH] = hx + ((x1 + col[r3 * DWT_PITCH]) >> 1);
+        }
+      }
+      __syncthreads();
+      }
+    }
+    // ---- write the 64x64 result
+    const int ow = min(DWT_T, L.rw - ox), oh = min(DWT_T, L.rh - oy);
+    for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
+      const int yy = i / DWT_T, xx = i % DWT_T;
+      if (yy < oh && xx < ow) out[(size_t)(oy + yy) * L.stride + ox + xx] = tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ output stage -------
+__device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
+__device__ __forceinline__ int lift_depth(int v, int in, int out) { return in >= out ? v >> (in - out) : v << (out - in); }
+
+// bytes per pixel and container depth of a reference OutputFormat
+__device__ __host__ __forceinline__ int fmt_bytes(int fmt) {
+  switch (fmt) {
+    case 0: return 4;
+    case 1: return 6;
+    case 2: return 3;
+    case 3: return 4;
+    case 4: return 8;
+    case 5: return 6;
+    case 6: return 3;
+    case 8: return 8;
+    default: return 0;
+  }
+}
+
+__device__ __forceinline__ void put_slot(uint8_t *px, int pxb, int slot, int v) {
+  // reference pixel structs store the highest component index first (codec_base.h:51-143)
+  if (pxb == 3) px[2 - slot] = (uint8_t)v;
+  else if (pxb == 4) px[3 - slot] = (uint8_t)v;
+  else if (pxb == 6) ((uint16_t *)px)[2 - slot] = (uint16_t)v;
+  else ((uint16_t *)px)[3 - slot] = (uint16_t)v;
+}
+
+// Inverse RCT / ICT + DC level shift + clamp + LIFT + pack (bmi_cpu_dwt_decoder.cpp
+// RICT_97_FLOAT :3570-3643, RRct_53 :3936-4130, MergeComponents :4283-4598).
+__global__ void __launch_bounds__(256) output_kernel(const OutGroup *__restrict__ groups,
+                                                     const OutTask *__restrict__ tasks, int ntasks, const void *bufA,
+                                                     const void *bufB, const void *bufC, uint8_t *out) {
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const OutTask tk = tasks[task];
+    const OutGroup G = groups[tk.group];
+    const int pxb = fmt_bytes(G.fmt);
+    const int B = G.bitdepth;
+    const int outdepth = (pxb == 3 || pxb == 4) ? 8 : 16;
+    const int maxv = (1 << B) - 1, dc = 1 << (B - 1);
+    const bool rgb = (G.fmt == 0 || G.fmt == 1 || G.fmt == 2 || G.fmt == 8);
+    const bool do_mct = rgb && G.mct && G.ncomp >= 3 && G.comp_buf[1] >= 0 && G.comp_buf[2] >= 0;
+    const int slot0 = (pxb == 4 || pxb == 8) ? 1 : 0;
+    const void *cb[4];
+    for (int c = 0; c < 4; ++c) {
+      const void *bb = G.comp_buf[c] == 0 ? bufA : (G.comp_buf[c] == 1 ? bufB : bufC);
+      cb[c] = G.comp_buf[c] < 0 ? nullptr : (const void *)((const uint8_t *)bb + G.comp_off[c] * 4);
+    }
+    const int ox = tk.tx * 64, oy = tk.ty * 64;
+    for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+      const int yy = oy + i / 64, xx = ox + i % 64;
+      if (yy >= G.h || xx >= G.w) continue;
+      uint8_t *px = out + G.out_off + ((size_t)(G.y0 + yy) * G.pitch_px + (G.x0 + xx)) * pxb;
+      uint8_t tmp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (do_mct) {
+        const size_t o0 = (size_t)yy * G.stride[0] + xx, o1 = (size_t)yy * G.stride[1] + xx,
+                     o2 = (size_t)yy * G.stride[2] + xx;
+        int v[3];
+        if (G.rev) {
+          const int y = ((const int32_t *)cb[0])[o0], u = ((const int32_t *)cb[1])[o1], w = ((const int32_t *)cb[2])[o2];
+          const int g = y - ((u + w) >> 2) + dc;
+          v[0] = clampi(w + g, maxv);
+          v[1] = clampi(g, maxv);
+          v[2] = clampi(u + g, maxv);
+        } else {
+          const float y = ((const float *)cb[0])[o0], u = ((const float *)cb[1])[o1], w = ((const float *)cb[2])[o2];
+          const float sh = (float)dc, fm = (float)maxv;
+          float t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.402f, w)), sh);
+          v[0] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+          t = __fadd_rn(__fadd_rn(__fadd_rn(y, __fmul_rn(-0.34413f, u)), __fmul_rn(-0.71414f, w)), sh);
+          v[1] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+          t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.772f, u)), sh);
+          v[2] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+        }
+        if (G.checkout >= 0 && G.checkout < 3) {
+          // one component replicated into R, G and B (RICT_97_FLOAT / RRct_53 case 0..2)
+          const int vv = lift_depth(v[G.checkout], B, outdepth);
+          for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k + slot0, vv);
+        } else {
+          for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k + slot0, lift_depth(v[k], B, outdepth));
+        }
+      } else if (G.checkout >= 0 && cb[G.checkout]) {
+        // MergeComponents with a checked-out component: value in R = G = B, and in the
+        // alpha slot only for the 4-component formats (bmi_cpu_dwt_decoder.cpp:4300-4308)
+        const size_t o = (size_t)yy * G.stride[G.checkout] + xx;
+        int v = G.rev ? ((const int32_t *)cb[G.checkout])[o] : (int)((const float *)cb[G.checkout])[o];
+        v = lift_depth(clampi(v + dc, maxv), B, outdepth);
+        if (pxb == 3 || pxb == 6) {
+          for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k, v);
+        } else {
+          for (int k = 1; k < 4; ++k) put_slot(tmp, pxb, k, v);
+          if (G.fmt == 3 || G.fmt == 4) put_slot(tmp, pxb, 0, v);
+        }
+      } else {
+        for (int c = 0; c < G.ncomp && c < 4; ++c) {
+          if (!cb[c]) continue;
+          if ((pxb == 3 || pxb == 6) && c > 2) continue;
+          const size_t o = (size_t)yy * G.stride[c] + xx;
+          int v = G.rev ? ((const int32_t *)cb[c])[o] : (int)((const float *)cb[c])[o];
+          v = clampi(v + dc, maxv);
+          put_slot(tmp, pxb, c, lift_depth(v, B, outdepth));
+        }
+      }
+      for (int k = 0; k < pxb; ++k) px[k] = tmp[k];
+    }
+  }
+}
+
+}  // namespace j2k_dev

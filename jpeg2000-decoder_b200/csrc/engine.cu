@@ -1,0 +1,793 @@
+/*
+ * engine.cu — device context, batching and the j2k_gpu C ABI (include/j2k_gpu.h).
+ *
+ * A batch is a set of decode plans.  batch_launch concatenates their Tier-1 work lists,
+ * coded bytes and DWT/output task tables into one pinned staging area, copies each
+ * section to the device with one cudaMemcpyAsync, then enqueues:
+ *   - Tier-1: one persistent launch per code-block size class (<= 32x32, <= 64x64) that
+ *     drains a work queue sorted by coded length (longest first);
+ *   - inverse DWT: one launch per level step for all tile-components of all images
+ *     (5/3 and 9/7 variants), coarsest level first;
+ *   - inverse MCT + DC shift + pack into each image's output;
+ *   - the per-block status back to the host.
+ * This replaces the reference's CudaManager job thread with its per-stripe H2D copies and
+ * per-component launch sequence (decoder/cudainterface/src/cudainterface.cpp:1072-1765,
+ * :2276-2640, gpulib.c:165-343).  There is no CPU fallback: without a device every call
+ * fails with J2K_ERR_NODEVICE.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include "../../include/j2k_gpu.h"
+#include "bmi_engine.h"
+#include "codestream.h"
+#include "dwt_kernel.cuh"
+#include "t1_kernel.cuh"
+
+using namespace j2k_dev;
+
+namespace {
+
+// ------------------------------------------------------------------ Tier-1 kernel -------
+__device__ __forceinline__ int32_t signmag_to_int(int32_t v) {
+  // FETCHPIXEL_INT, bmi_cpu_dwt_decoder.cpp:2287
+  return (v & 0x80000000) ? ((v - 1) ^ 0x7FFFFFFF) : (v & 0x7FFFFFFF);
+}
+__device__ __forceinline__ int32_t place53(int32_t v, int numbps) {
+  // dec_t1_comp.cpp:341-366
+  int sh = 31 - numbps;
+  sh = sh < 0 ? 0 : (sh > 31 ? 31 : sh);
+  return v < 0 ? -(int32_t)((uint32_t)(v & 0x7FFFFFFF) >> sh) : (int32_t)((uint32_t)v >> sh);
+}
+
+template <int MAXW, int MAXH>
+struct T1Layout {
+  static constexpr int STRIPES = MAXH / 4;
+  static constexpr int GAP = MAXW + 3;
+  static constexpr int CWN = (STRIPES + 2) * GAP + 2;
+  static constexpr int PER_WARP = ((CWN * 4 + MAXH * MAXW * 4 + 32) + 15) & ~15;
+};
+
+template <int MAXW, int MAXH>
+__global__ void t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n,
+                          int *__restrict__ counter, const uint8_t *__restrict__ bytes,
+                          const uint32_t *__restrict__ seglens, void *__restrict__ coef, uint16_t *__restrict__ status,
+                          const T1Tables *__restrict__ gtab) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  typedef T1Layout<MAXW, MAXH> Lay;
+  T1Tables &T = *reinterpret_cast<T1Tables *>(smem);
+  for (int i = threadIdx.x; i < (int)(sizeof(T1Tables) / 4); i += blockDim.x)
+    reinterpret_cast<uint32_t *>(smem)[i] = reinterpret_cast<const uint32_t *>(gtab)[i];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t *mine = smem + ((sizeof(T1Tables) + 15) & ~15) + warp * Lay::PER_WARP;
+  BlockSmem b;
+  b.cw = reinterpret_cast<uint32_t *>(mine);
+  b.sp = reinterpret_cast<int32_t *>(mine + Lay::CWN * 4);
+  b.st = mine + Lay::CWN * 4 + MAXH * MAXW * 4;
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(counter, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= n) break;
+    const uint32_t ci = order[idx];
+    const j2k_cblk cb = cbs[ci];
+    b.w = cb.w;
+    b.gap = cb.w + 3;
+    int st;
+    if (cb.w == 0 || cb.h == 0 || cb.w > MAXW || cb.h > MAXH) {
+      st = 9;
+    } else {
+      st = decode_block<MAXW, MAXH>(cb, bytes, seglens, b, T, lane);
+    }
+    // dequantising (9/7) or shifting (5/3) store into the subband buffer, coalesced by row
+    const int w = cb.w, h = cb.h;
+    if (st != 9) {
+      if (cb.flags & J2K_CB_IRREV) {
+        float *dst = reinterpret_cast<float *>(coef) + cb.out_off;
+        for (int i = lane; i < w * h; i += 32) {
+          const int y = i / w, x = i - y * w;
+          dst[(size_t)y * cb.out_stride + x] = __fmul_rn((float)signmag_to_int(b.sp[y * w + x]), cb.gain);
+        }
+      } else {
+        int32_t *dst = reinterpret_cast<int32_t *>(coef) + cb.out_off;
+        for (int i = lane; i < w * h; i += 32) {
+          const int y = i / w, x = i - y * w;
+          dst[(size_t)y * cb.out_stride + x] = place53(b.sp[y * w + x], cb.mb);
+        }
+      }
+    }
+    if (lane == 0) status[ci] = (uint16_t)st;
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------------ host tables --------
+void build_t1_tables(T1Tables &T) {
+  static const uint16_t QE[47] = {0x5601, 0x3401, 0x1801, 0x0AC1, 0x0521, 0x0221, 0x5601, 0x5401, 0x4801, 0x3801,
+                                  0x3001, 0x2401, 0x1C01, 0x1601, 0x5601, 0x5401, 0x5101, 0x4801, 0x3801, 0x3401,
+                                  0x3001, 0x2801, 0x2401, 0x2201, 0x1C01, 0x1801, 0x1601, 0x1401, 0x1201, 0x1101,
+                                  0x0AC1, 0x09C1, 0x08A1, 0x0521, 0x0441, 0x02A1, 0x0221, 0x0141, 0x0111, 0x0085,
+                                  0x0049, 0x0025, 0x0015, 0x0009, 0x0005, 0x0001, 0x5601};
+  static const uint8_t NMPS[47] = {1,  2,  3,  4,  5,  38, 7,  8,  9,  10, 11, 12, 13, 29, 15, 16,
+                                   17, 18, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 32,
+                                   33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 44, 45, 45, 46};
+  static const uint8_t NLPS[47] = {1,  6,  9,  12, 29, 33, 6,  14, 14, 14, 17, 18, 20, 21, 14, 14,
+                                   15, 16, 17, 18, 19, 19, 20, 21, 22, 23, 24, 25, 26, 27, 28, 29,
+                                   30, 31, 32, 33, 34, 35, 36, 37, 38, 39, 40, 41, 42, 43, 46};
+  std::memset(&T, 0, sizeof(T));
+  for (int s = 0; s < 94; ++s) {
+    int idx = s >> 1, mps = s & 1;
+    int sw = (QE[idx] == 0x5601 && NLPS[idx] != 46);
+    uint32_t nm = (uint32_t)(NMPS[idx] << 1 | mps);
+    uint32_t nl = (uint32_t)(NLPS[idx] << 1 | (mps ^ sw));
+    T.mq[s] = ((uint32_t)QE[idx] << 16) | (nm << 8) | nl;
+  }
+  for (int band = 0; band < 3; ++band)
+    for (int nb = 0; nb < 512; ++nb) {
+      int h = ((nb >> 3) & 1) + ((nb >> 5) & 1);
+      int v = ((nb >> 1) & 1) + ((nb >> 7) & 1);
+      int d = (nb & 1) + ((nb >> 2) & 1) + ((nb >> 6) & 1) + ((nb >> 8) & 1);
+      int c;
+      if (band == 2) {  // HH
+        int hv = h + v;
+        if (d >= 3) c = 8;
+        else if (d == 2) c = hv >= 1 ? 7 : 6;
+        else if (d == 1) c = hv >= 2 ? 5 : (hv == 1 ? 4 : 3);
+        else c = hv >= 2 ? 2 : hv;
+      } else {
+        if (band == 1) std::swap(h, v);  // HL
+        if (h == 2) c = 8;
+        else if (h == 1) c = v >= 1 ? 7 : (d >= 1 ? 6 : 5);
+        else if (v == 2) c = 4;
+        else if (v == 1) c = 3;
+        else c = d >= 2 ? 2 : d;
+      }
+      T.zc[band][nb] = (uint8_t)c;
+    }
+  for (int i = 0; i < 256; ++i) {
+    // bit 0 sigma up, 1 chi up, 2 sigma down, 3 chi down, 4 sigma left, 5 chi left,
+    // 6 sigma right, 7 chi right (T.800 Table D.3)
+    auto contrib = [&](int sb, int xb) { return ((i >> sb) & 1) ? (((i >> xb) & 1) ? -1 : 1) : 0; };
+    int H = contrib(4, 5) + contrib(6, 7);
+    int V = contrib(0, 1) + contrib(2, 3);
+    H = std::max(-1, std::min(1, H));
+    V = std::max(-1, std::min(1, V));
+    int x = 0;
+    if (H < 0 || (H == 0 && V < 0)) {
+      H = -H;
+      V = -V;
+      x = 1;
+    }
+    int c = (H == 1) ? (V == 1 ? 4 : (V == 0 ? 3 : 2)) : (V == 1 ? 1 : 0);
+    T.sc[i] = (uint8_t)(c << 1 | x);
+  }
+}
+
+// ------------------------------------------------------------------ device buffers -----
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+struct BatchImage {
+  const j2k_plan *plan;
+  int fmt, flags;
+  int checkout;
+  uint64_t coef_base, out_base, out_bytes;
+  uint32_t cblk_base;
+  int status, bad;
+};
+
+}  // namespace
+
+struct j2k_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr, user_stream = nullptr;
+  size_t budget = 0, reserved = 0;
+  DevBuf d_bytes, d_cblks, d_order, d_seg, d_status, d_counter, d_A, d_B, d_C, d_levels, d_dtasks, d_groups, d_otasks,
+      d_out, d_tables;
+  void *h_stage = nullptr;
+  size_t h_stage_cap = 0;
+  std::vector<BatchImage> imgs;
+  uint16_t *h_status = nullptr;  // pinned
+  size_t h_status_cap = 0;
+  bool launched = false, synced = false;
+  cudaEvent_t ev[6] = {};
+  float t_t1 = 0, t_dwt = 0, t_h2d = 0, t_total = 0;
+  int launches = 0;
+  j2k_gpu_tuning tuning{8, 64, 0};
+  int sm_count = 148;
+  size_t smem_optin = 227 * 1024;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e) {
+  (void)e;
+  return J2K_ERR_CUDA;
+}
+
+#define CK(x)                                  \
+  do {                                         \
+    cudaError_t _e = (x);                      \
+    if (_e != cudaSuccess) return cuda_fail(_e); \
+  } while (0)
+
+int ensure(j2k_gpu_ctx *c, DevBuf &b, size_t need) {
+  if (need == 0) need = 16;
+  if (b.cap >= need) return J2K_OK;
+  size_t nc = std::max(need, b.cap + b.cap / 2);
+  if (c->reserved - b.cap + nc > c->budget) {
+    nc = need;
+    if (c->reserved - b.cap + nc > c->budget) return J2K_ERR_NOMEM;
+  }
+  if (b.p) {
+    cudaFree(b.p);
+    c->reserved -= b.cap;
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  cudaError_t e = cudaMalloc(&b.p, nc);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return J2K_ERR_NOMEM;
+  }
+  b.cap = nc;
+  c->reserved += nc;
+  return J2K_OK;
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+}  // namespace
+
+extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **out) {
+  if (!out) return J2K_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return J2K_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= n) return J2K_ERR_ARG;
+  j2k_gpu_ctx *c = new (std::nothrow) j2k_gpu_ctx;
+  if (!c) return J2K_ERR_NOMEM;
+  c->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete c;
+    return J2K_ERR_CUDA;
+  }
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  c->budget = mem_budget ? mem_budget : (size_t)(fr * 0.8);
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) {
+    c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = prop.sharedMemPerBlockOptin;
+  }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return J2K_ERR_CUDA;
+  }
+  for (auto &e : c->ev) cudaEventCreate(&e);
+  T1Tables T;
+  build_t1_tables(T);
+  if (ensure(c, c->d_tables, sizeof(T1Tables)) != J2K_OK ||
+      cudaMemcpy(c->d_tables.p, &T, sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+    j2k_gpu_ctx_destroy(c);
+    return J2K_ERR_CUDA;
+  }
+  // opt into the large dynamic shared memory of the Tier-1 kernels
+  cudaFuncSetAttribute(t1_kernel<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  *out = c;
+  return J2K_OK;
+}
+
+extern "C" void j2k_gpu_ctx_destroy(j2k_gpu_ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DevBuf *all[] = {&c->d_bytes, &c->d_cblks, &c->d_order, &c->d_seg,    &c->d_status, &c->d_counter,
+                   &c->d_A,     &c->d_B,     &c->d_C,     &c->d_levels, &c->d_dtasks, &c->d_groups,
+                   &c->d_otasks, &c->d_out,  &c->d_tables};
+  for (DevBuf *b : all)
+    if (b->p) cudaFree(b->p);
+  if (c->h_stage) cudaFreeHost(c->h_stage);
+  if (c->h_status) cudaFreeHost(c->h_status);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" int j2k_gpu_mem_usage(const j2k_gpu_ctx *c, size_t *reserved, size_t *budget) {
+  if (!c) return J2K_ERR_ARG;
+  if (reserved) *reserved = c->reserved;
+  if (budget) *budget = c->budget;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_set_tuning(j2k_gpu_ctx *c, const j2k_gpu_tuning *t) {
+  if (!c || !t) return J2K_ERR_ARG;
+  j2k_gpu_tuning n = *t;
+  if (n.t1_warps_per_cta <= 0) n.t1_warps_per_cta = 8;
+  if (n.t1_warps_per_cta > 32) n.t1_warps_per_cta = 32;
+  if (n.dwt_tile <= 0) n.dwt_tile = 64;
+  c->tuning = n;
+  return J2K_OK;
+}
+extern "C" int j2k_gpu_get_tuning(const j2k_gpu_ctx *c, j2k_gpu_tuning *t) {
+  if (!c || !t) return J2K_ERR_ARG;
+  *t = c->tuning;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_batch_begin(j2k_gpu_ctx *c) {
+  if (!c) return J2K_ERR_ARG;
+  if (c->launched && !c->synced) return J2K_ERR_STATE;
+  c->imgs.clear();
+  c->launched = c->synced = false;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_batch_add(j2k_gpu_ctx *c, const j2k_plan *plan, int fmt, int flags, int *slot) {
+  if (!c || !plan) return J2K_ERR_ARG;
+  if (c->launched) return J2K_ERR_STATE;
+  if (fmt != J2K_FMT_NONE && j2k_dev::fmt_bytes(fmt) == 0) return J2K_ERR_ARG;
+  const j2k_image_info &I = plan->p.info;
+  if (I.bitdepth < 1 || I.bitdepth > 16) return J2K_ERR_UNSUPPORTED;
+  BatchImage bi{};
+  bi.checkout = -1;
+  bi.plan = plan;
+  bi.fmt = fmt;
+  bi.flags = flags;
+  if (slot) *slot = (int)c->imgs.size();
+  c->imgs.push_back(bi);
+  return J2K_OK;
+}
+
+namespace {
+
+struct Sizes {
+  size_t bytes = 0, cblks = 0, segs = 0, coef = 0, out = 0;
+};
+
+Sizes batch_sizes(j2k_gpu_ctx *c) {
+  Sizes s;
+  for (auto &im : c->imgs) {
+    const auto &p = im.plan->p;
+    im.coef_base = s.coef;
+    im.cblk_base = (uint32_t)s.cblks;
+    im.out_base = align_up(s.out, 256);
+    im.out_bytes = im.fmt == J2K_FMT_NONE ? 0 : j2k_output_bytes(&p.info, im.fmt);
+    s.bytes += p.bytes.size();
+    s.cblks += p.cblks.size();
+    s.segs += p.seglens.size();
+    s.coef += p.info.coef_elems;
+    s.out = im.out_base + im.out_bytes;
+  }
+  return s;
+}
+
+}  // namespace
+
+extern "C" int j2k_gpu_batch_footprint(const j2k_gpu_ctx *cc, size_t *bytes) {
+  if (!cc || !bytes) return J2K_ERR_ARG;
+  j2k_gpu_ctx *c = const_cast<j2k_gpu_ctx *>(cc);
+  Sizes s = batch_sizes(c);
+  *bytes = s.bytes + s.cblks * (sizeof(j2k_cblk) + 4 + 2) + s.segs * 4 + s.coef * 12 + s.out;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_batch_launch(j2k_gpu_ctx *c, void *user_stream) {
+  if (!c) return J2K_ERR_ARG;
+  if (c->launched) return J2K_ERR_STATE;
+  if (c->imgs.empty()) return J2K_ERR_STATE;
+  cudaSetDevice(c->device);
+  cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
+  c->user_stream = st;
+  Sizes S = batch_sizes(c);
+
+  // ---- host task tables
+  std::vector<j2k_cblk> cbs;
+  cbs.reserve(S.cblks);
+  std::vector<uint32_t> seg;
+  seg.reserve(S.segs);
+  std::vector<uint32_t> ord_big, ord_small;
+  std::vector<DwtLevel> levels;
+  std::vector<std::vector<DwtTask>> steps_rev, steps_irr;
+  std::vector<OutGroup> groups;
+  std::vector<OutTask> otasks;
+  uint64_t byte_base = 0;
+  uint32_t seg_base = 0;
+  int maxL = 0;
+  for (auto &im : c->imgs)
+    for (auto &tc : im.plan->p.tilecomps) maxL = std::max(maxL, tc.levels);
+  steps_rev.resize(maxL);
+  steps_irr.resize(maxL);
+  for (auto &im : c->imgs) {
+    const auto &p = im.plan->p;
+    for (const j2k_cblk &cb0 : p.cblks) {
+      j2k_cblk cb = cb0;
+      cb.data_off = (uint32_t)(cb.data_off + byte_base);
+      cb.seg_off += seg_base;
+      cb.out_off += im.coef_base;
+      cb.status = 0;
+      uint32_t idx = (uint32_t)cbs.size();
+      cbs.push_back(cb);
+      if (cb.num_passes == 0 && !(cb.flags & J2K_CB_IRREV) && false) continue;
+      if (cb.w <= 32 && cb.h <= 32) ord_small.push_back(idx);
+      else ord_big.push_back(idx);
+    }
+    seg.insert(seg.end(), p.seglens.begin(), p.seglens.end());
+    byte_base += p.bytes.size();
+    seg_base += (uint32_t)p.seglens.size();
+    const bool rev = p.info.reversible != 0;
+    const int refc = (im.flags & J2K_FLAG_REF_COMPAT) ? 1 : 0;
+    // DWT levels of every tile-component, aligned so that all finish at the last step
+    std::vector<int8_t> final_buf(p.tilecomps.size());
+    for (size_t t = 0; t < p.tilecomps.size(); ++t) {
+      const j2k_tilecomp &tc = p.tilecomps[t];
+      const int Lt = tc.levels;
+      final_buf[t] = Lt == 0 ? 0 : ((Lt & 1) ? 1 : 2);
+      for (int r = 1; r <= Lt; ++r) {
+        DwtLevel L{};
+        L.base = im.coef_base + tc.coef_off;
+        L.stride = tc.w;
+        L.rw = tc.res_w[r];
+        L.rh = tc.res_h[r];
+        L.lw = tc.res_w[r - 1];
+        L.lh = tc.res_h[r - 1];
+        L.ll_src = r == 1 ? 0 : (((r - 1) & 1) ? 1 : 2);
+        L.out_dst = (r & 1) ? 1 : 2;
+        L.ll_gain = (!rev && r > 1) ? 1 : 0;
+        L.refcompat = (int8_t)refc;
+        if (L.rw <= 0 || L.rh <= 0) continue;
+        L.tiles_x = (L.rw + DWT_T - 1) / DWT_T;
+        const int tiles_y = (L.rh + DWT_T - 1) / DWT_T;
+        const uint32_t li = (uint32_t)levels.size();
+        levels.push_back(L);
+        const int step = maxL - Lt + r - 1;
+        auto &dst = rev ? steps_rev[step] : steps_irr[step];
+        for (int ty = 0; ty < tiles_y; ++ty)
+          for (int tx = 0; tx < L.tiles_x; ++tx) dst.push_back({li, (uint16_t)tx, (uint16_t)ty});
+      }
+    }
+    if (im.fmt != J2K_FMT_NONE) {
+      // output groups: one per tile
+      for (size_t t = 0; t < p.tilecomps.size(); ++t) {
+        const j2k_tilecomp &tc = p.tilecomps[t];
+        if (tc.comp != 0) continue;
+        OutGroup G{};
+        for (int k = 0; k < 4; ++k) G.comp_buf[k] = -1;
+        int nc = 0;
+        for (size_t u = 0; u < p.tilecomps.size(); ++u) {
+          const j2k_tilecomp &tu = p.tilecomps[u];
+          if (tu.tile != tc.tile || tu.comp >= 4) continue;
+          G.comp_off[tu.comp] = im.coef_base + tu.coef_off;
+          G.comp_buf[tu.comp] = final_buf[u];
+          G.stride[tu.comp] = tu.w;
+          nc = std::max(nc, tu.comp + 1);
+        }
+        G.x0 = tc.x0;
+        G.y0 = tc.y0;
+        G.w = tc.w;
+        G.h = tc.h;
+        G.out_off = im.out_base;
+        G.pitch_px = p.info.width;
+        G.fmt = (int16_t)im.fmt;
+        G.bitdepth = (int16_t)p.info.bitdepth;
+        G.rev = (int8_t)rev;
+        G.mct = (int8_t)p.info.mct;
+        G.ncomp = (int8_t)nc;
+        G.checkout = (int8_t)((im.checkout >= 0 && im.checkout < nc) ? im.checkout : -1);
+        G.tiles_x = (tc.w + 63) / 64;
+        const uint32_t gi = (uint32_t)groups.size();
+        groups.push_back(G);
+        for (int ty = 0; ty < (tc.h + 63) / 64; ++ty)
+          for (int tx = 0; tx < G.tiles_x; ++tx) otasks.push_back({gi, (uint16_t)tx, (uint16_t)ty});
+      }
+    }
+  }
+  // work queue order: longest coded length first
+  auto by_len = [&](uint32_t a, uint32_t b) { return cbs[a].data_len > cbs[b].data_len; };
+  std::sort(ord_big.begin(), ord_big.end(), by_len);
+  std::sort(ord_small.begin(), ord_small.end(), by_len);
+  std::vector<uint32_t> dtask_off(2 * maxL + 1, 0);
+  std::vector<DwtTask> dtasks;
+  for (int s = 0; s < maxL; ++s) {
+    dtask_off[2 * s] = (uint32_t)dtasks.size();
+    dtasks.insert(dtasks.end(), steps_rev[s].begin(), steps_rev[s].end());
+    dtask_off[2 * s + 1] = (uint32_t)dtasks.size();
+    dtasks.insert(dtasks.end(), steps_irr[s].begin(), steps_irr[s].end());
+  }
+  dtask_off[2 * maxL] = (uint32_t)dtasks.size();
+
+  // ---- staging layout (pinned)
+  size_t o_cbs = 0;
+  size_t o_ord = align_up(o_cbs + cbs.size() * sizeof(j2k_cblk), 256);
+  size_t o_seg = align_up(o_ord + (ord_big.size() + ord_small.size()) * 4, 256);
+  size_t o_lev = align_up(o_seg + seg.size() * 4, 256);
+  size_t o_dtk = align_up(o_lev + levels.size() * sizeof(DwtLevel), 256);
+  size_t o_grp = align_up(o_dtk + dtasks.size() * sizeof(DwtTask), 256);
+  size_t o_otk = align_up(o_grp + groups.size() * sizeof(OutGroup), 256);
+  size_t o_byt = align_up(o_otk + otasks.size() * sizeof(OutTask), 256);
+  size_t total = align_up(o_byt + S.bytes + 16, 256);
+  if (c->h_stage_cap < total) {
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    c->h_stage = nullptr;
+    c->h_stage_cap = 0;
+    size_t nc = std::max(total, c->h_stage_cap * 3 / 2);
+    if (cudaMallocHost(&c->h_stage, nc) != cudaSuccess) {
+      cudaGetLastError();
+      return J2K_ERR_NOMEM;
+    }
+    c->h_stage_cap = nc;
+  }
+  uint8_t *H = (uint8_t *)c->h_stage;
+  std::memcpy(H + o_cbs, cbs.data(), cbs.size() * sizeof(j2k_cblk));
+  std::memcpy(H + o_ord, ord_big.data(), ord_big.size() * 4);
+  std::memcpy(H + o_ord + ord_big.size() * 4, ord_small.data(), ord_small.size() * 4);
+  std::memcpy(H + o_seg, seg.data(), seg.size() * 4);
+  std::memcpy(H + o_lev, levels.data(), levels.size() * sizeof(DwtLevel));
+  std::memcpy(H + o_dtk, dtasks.data(), dtasks.size() * sizeof(DwtTask));
+  std::memcpy(H + o_grp, groups.data(), groups.size() * sizeof(OutGroup));
+  std::memcpy(H + o_otk, otasks.data(), otasks.size() * sizeof(OutTask));
+  {
+    size_t off = o_byt;
+    for (auto &im : c->imgs) {
+      const auto &b = im.plan->p.bytes;
+      if (!b.empty()) std::memcpy(H + off, b.data(), b.size());
+      off += b.size();
+    }
+  }
+
+  // ---- device buffers
+  int rc;
+  if ((rc = ensure(c, c->d_cblks, o_byt)) != J2K_OK) return rc;  // all tables in one block
+  if ((rc = ensure(c, c->d_bytes, S.bytes + 16)) != J2K_OK) return rc;
+  if ((rc = ensure(c, c->d_status, S.cblks * 2 + 16)) != J2K_OK) return rc;
+  if ((rc = ensure(c, c->d_counter, 64)) != J2K_OK) return rc;
+  if ((rc = ensure(c, c->d_A, S.coef * 4 + 16)) != J2K_OK) return rc;
+  if ((rc = ensure(c, c->d_B, S.coef * 4 + 16)) != J2K_OK) return rc;
+  if ((rc = ensure(c, c->d_C, S.coef * 4 + 16)) != J2K_OK) return rc;
+  if ((rc = ensure(c, c->d_out, S.out + 16)) != J2K_OK) return rc;
+  uint8_t *D = (uint8_t *)c->d_cblks.p;
+  c->launches = 0;
+
+  CK(cudaEventRecord(c->ev[0], st));
+  CK(cudaMemcpyAsync(D, H, o_byt, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_bytes.p, H + o_byt, S.bytes, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(c->d_counter.p, 0, 64, st));
+  CK(cudaEventRecord(c->ev[1], st));
+
+  // ---- Tier-1
+  const j2k_cblk *d_cbs = (const j2k_cblk *)(D + o_cbs);
+  const uint32_t *d_ord = (const uint32_t *)(D + o_ord);
+  const uint32_t *d_seg = (const uint32_t *)(D + o_seg);
+  int *cnt = (int *)c->d_counter.p;
+  const T1Tables *tab = (const T1Tables *)c->d_tables.p;
+  const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
+  if (!ord_big.empty()) {
+    int warps = std::max(1, std::min(c->tuning.t1_warps_per_cta, (int)((c->smem_optin - tsz) / T1Layout<64, 64>::PER_WARP)));
+    size_t sm = tsz + (size_t)warps * T1Layout<64, 64>::PER_WARP;
+    int ctas_per_sm = std::max(1, (int)((228 * 1024) / (sm + 1024)));
+    int grid = std::min((int)((ord_big.size() + warps - 1) / warps), c->sm_count * ctas_per_sm);
+    t1_kernel<64, 64><<<grid, warps * 32, sm, st>>>(d_cbs, d_ord, (int)ord_big.size(), cnt, (const uint8_t *)c->d_bytes.p,
+                                                     d_seg, c->d_A.p, (uint16_t *)c->d_status.p, tab);
+    c->launches++;
+  }
+  if (!ord_small.empty()) {
+    int warps = std::max(1, std::min(2 * c->tuning.t1_warps_per_cta, 32));
+    size_t sm = tsz + (size_t)warps * T1Layout<32, 32>::PER_WARP;
+    while (sm > c->smem_optin && warps > 1) {
+      warps /= 2;
+      sm = tsz + (size_t)warps * T1Layout<32, 32>::PER_WARP;
+    }
+    int ctas_per_sm = std::max(1, (int)((228 * 1024) / (sm + 1024)));
+    int grid = std::min((int)((ord_small.size() + warps - 1) / warps), c->sm_count * ctas_per_sm);
+    t1_kernel<32, 32><<<grid, warps * 32, sm, st>>>(d_cbs, d_ord + ord_big.size(), (int)ord_small.size(), cnt + 1,
+                                                     (const uint8_t *)c->d_bytes.p, d_seg, c->d_A.p,
+                                                     (uint16_t *)c->d_status.p, tab);
+    c->launches++;
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[2], st));
+
+  // ---- inverse DWT, coarsest level step first
+  const DwtLevel *d_lev = (const DwtLevel *)(D + o_lev);
+  const DwtTask *d_dtk = (const DwtTask *)(D + o_dtk);
+  const float llg = j2k::irrev_ll_gain();
+  const int dwt_cap = c->sm_count * 8;
+  for (int s = 0; s < maxL; ++s) {
+    int n_rev = (int)(dtask_off[2 * s + 1] - dtask_off[2 * s]);
+    int n_irr = (int)(dtask_off[2 * s + 2] - dtask_off[2 * s + 1]);
+    if (n_rev) {
+      dwt_level_kernel<true><<<std::min(n_rev, dwt_cap), 256, 0, st>>>(d_lev, d_dtk + dtask_off[2 * s], n_rev, c->d_A.p,
+                                                                        c->d_B.p, c->d_C.p, llg);
+      c->launches++;
+    }
+    if (n_irr) {
+      dwt_level_kernel<false><<<std::min(n_irr, dwt_cap), 256, 0, st>>>(d_lev, d_dtk + dtask_off[2 * s + 1], n_irr,
+                                                                         c->d_A.p, c->d_B.p, c->d_C.p, llg);
+      c->launches++;
+    }
+  }
+  if (!otasks.empty()) {
+    output_kernel<<<std::min((int)otasks.size(), dwt_cap), 256, 0, st>>>(
+        (const OutGroup *)(D + o_grp), (const OutTask *)(D + o_otk), (int)otasks.size(), c->d_A.p, c->d_B.p, c->d_C.p,
+        (uint8_t *)c->d_out.p);
+    c->launches++;
+  }
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->ev[3], st));
+  if (c->h_status_cap < S.cblks + 1) {
+    if (c->h_status) cudaFreeHost(c->h_status);
+    c->h_status = nullptr;
+    c->h_status_cap = 0;
+    if (cudaMallocHost(&c->h_status, (S.cblks + 1) * 2) != cudaSuccess) {
+      cudaGetLastError();
+      return J2K_ERR_NOMEM;
+    }
+    c->h_status_cap = S.cblks + 1;
+  }
+  if (S.cblks) CK(cudaMemcpyAsync(c->h_status, c->d_status.p, S.cblks * 2, cudaMemcpyDeviceToHost, st));
+  CK(cudaEventRecord(c->ev[4], st));
+  c->launched = true;
+  c->synced = false;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_batch_sync(j2k_gpu_ctx *c, int timeout_ms) {
+  if (!c) return J2K_ERR_ARG;
+  if (!c->launched) return J2K_ERR_STATE;
+  if (c->synced) return J2K_OK;
+  cudaSetDevice(c->device);
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaEventQuery(c->ev[4]);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) return J2K_ERR_CUDA;
+    if (timeout_ms >= 0) {
+      auto el = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+      if (el > timeout_ms) return J2K_ERR_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  cudaEventElapsedTime(&c->t_h2d, c->ev[0], c->ev[1]);
+  cudaEventElapsedTime(&c->t_t1, c->ev[1], c->ev[2]);
+  cudaEventElapsedTime(&c->t_dwt, c->ev[2], c->ev[3]);
+  cudaEventElapsedTime(&c->t_total, c->ev[0], c->ev[4]);
+  for (auto &im : c->imgs) {
+    int bad = 0;
+    const size_t n = im.plan->p.cblks.size();
+    for (size_t i = 0; i < n; ++i)
+      if (c->h_status[im.cblk_base + i]) bad++;
+    im.bad = bad;
+    im.status = bad ? J2K_ERR_DECODE : J2K_OK;
+  }
+  c->synced = true;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_image_status(const j2k_gpu_ctx *c, int slot, int *bad) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size()) return J2K_ERR_ARG;
+  if (!c->synced) return J2K_ERR_STATE;
+  if (bad) *bad = c->imgs[slot].bad;
+  return c->imgs[slot].status;
+}
+
+extern "C" int j2k_gpu_output_device(const j2k_gpu_ctx *c, int slot, const void **dptr, size_t *bytes) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size() || !dptr) return J2K_ERR_ARG;
+  if (!c->launched) return J2K_ERR_STATE;
+  *dptr = (const uint8_t *)c->d_out.p + c->imgs[slot].out_base;
+  if (bytes) *bytes = c->imgs[slot].out_bytes;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_output_copy(j2k_gpu_ctx *c, int slot, void *dst, size_t bytes) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size() || !dst) return J2K_ERR_ARG;
+  if (!c->synced) return J2K_ERR_STATE;
+  const BatchImage &im = c->imgs[slot];
+  if (bytes < im.out_bytes) return J2K_ERR_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaMemcpyAsync(dst, (const uint8_t *)c->d_out.p + im.out_base, im.out_bytes, cudaMemcpyDeviceToHost,
+                     c->user_stream));
+  CK(cudaStreamSynchronize(c->user_stream));
+  return J2K_OK;
+}
+
+namespace {
+// copy a tile-component region of buffer `buf` to the host
+int copy_region(j2k_gpu_ctx *c, const void *buf, uint64_t off, size_t elems, void *dst) {
+  CK(cudaMemcpyAsync(dst, (const uint8_t *)buf + off * 4, elems * 4, cudaMemcpyDeviceToHost, c->user_stream));
+  return J2K_OK;
+}
+}  // namespace
+
+extern "C" int j2k_gpu_coefficients_copy(j2k_gpu_ctx *c, int slot, int stage, void *dst, size_t bytes) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size() || !dst) return J2K_ERR_ARG;
+  if (!c->synced) return J2K_ERR_STATE;
+  const BatchImage &im = c->imgs[slot];
+  const auto &p = im.plan->p;
+  if (bytes < p.info.coef_elems * 4) return J2K_ERR_ARG;
+  cudaSetDevice(c->device);
+  for (const j2k_tilecomp &tc : p.tilecomps) {
+    const int Lt = tc.levels;
+    const void *buf = c->d_A.p;
+    if (stage == 1 && Lt > 0) buf = (Lt & 1) ? c->d_B.p : c->d_C.p;
+    int rc = copy_region(c, buf, im.coef_base + tc.coef_off, (size_t)tc.w * tc.h, (uint8_t *)dst + tc.coef_off * 4);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(c->user_stream));
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_component_copy(j2k_gpu_ctx *c, int slot, int comp, void *dst, size_t bytes) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size() || !dst) return J2K_ERR_ARG;
+  if (!c->synced) return J2K_ERR_STATE;
+  const BatchImage &im = c->imgs[slot];
+  const auto &p = im.plan->p;
+  const size_t need = (size_t)p.info.width * p.info.height * 4;
+  if (bytes < need || comp < 0 || comp >= p.info.ncomp) return J2K_ERR_ARG;
+  cudaSetDevice(c->device);
+  bool found = false;
+  for (const j2k_tilecomp &tc : p.tilecomps) {
+    if (tc.comp != comp) continue;
+    found = true;
+    const int Lt = tc.levels;
+    const void *buf = Lt == 0 ? c->d_A.p : ((Lt & 1) ? c->d_B.p : c->d_C.p);
+    CK(cudaMemcpy2DAsync((uint8_t *)dst + ((size_t)tc.y0 * p.info.width + tc.x0) * 4, (size_t)p.info.width * 4,
+                         (const uint8_t *)buf + (im.coef_base + tc.coef_off) * 4, (size_t)tc.w * 4, (size_t)tc.w * 4,
+                         tc.h, cudaMemcpyDeviceToHost, c->user_stream));
+  }
+  if (!found) return J2K_ERR_ARG;
+  CK(cudaStreamSynchronize(c->user_stream));
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_last_timing(const j2k_gpu_ctx *c, float *t1, float *dwt, float *h2d, float *total) {
+  if (!c || !c->synced) return J2K_ERR_STATE;
+  if (t1) *t1 = c->t_t1;
+  if (dwt) *dwt = c->t_dwt;
+  if (h2d) *h2d = c->t_h2d;
+  if (total) *total = c->t_total;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_last_launches(const j2k_gpu_ctx *c, int *n) {
+  if (!c || !n) return J2K_ERR_ARG;
+  *n = c->launches;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_decode(j2k_gpu_ctx *c, const uint8_t *cs, size_t len, int fmt, int flags, void *host_out,
+                              size_t host_out_bytes) {
+  if (!c || !cs || !host_out) return J2K_ERR_ARG;
+  j2k_plan *p = nullptr;
+  int rc = j2k_plan_create(cs, len, 0, 0, 0, &p);
+  if (rc) return rc;
+  if ((rc = j2k_gpu_batch_begin(c)) == J2K_OK && (rc = j2k_gpu_batch_add(c, p, fmt, flags, nullptr)) == J2K_OK &&
+      (rc = j2k_gpu_batch_launch(c, nullptr)) == J2K_OK && (rc = j2k_gpu_batch_sync(c, -1)) == J2K_OK) {
+    rc = j2k_gpu_output_copy(c, 0, host_out, host_out_bytes);
+    if (rc == J2K_OK) rc = j2k_gpu_image_status(c, 0, nullptr);
+  }
+  j2k_gpu_batch_begin(c);
+  j2k_plan_destroy(p);
+  return rc;
+}
+
+int bmi_engine::set_checkout(j2k_gpu_ctx *c, int slot, int comp) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size()) return J2K_ERR_ARG;
+  if (c->launched) return J2K_ERR_STATE;
+  c->imgs[slot].checkout = comp;
+  return J2K_OK;
+}

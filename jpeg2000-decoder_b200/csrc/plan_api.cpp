@@ -7,10 +7,6 @@
 #include "../../include/j2k_gpu.h"
 #include "codestream.h"
 
-struct j2k_plan {
-  j2k::ImagePlan p;
-};
-
 extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels, int max_layers,
                                unsigned ignore_components, j2k_plan **out) {
   if (!cs || !out || len < 2) return J2K_ERR_ARG;

@@ -1,0 +1,481 @@
+/*
+ * t1_kernel.cuh — EBCOT Tier-1 code-block decoder for sm_100a.
+ *
+ * One warp per code-block.  The warp keeps the block's stripe context words and its int32
+ * samples in shared memory and the MQ registers (A, C, t, T, byte position) in registers.
+ * The arithmetic decode is inherently serial, so all 32 lanes execute the same scalar
+ * decode in lock-step (uniform control flow, broadcast shared-memory reads); the lanes
+ * work in parallel where the data allows it: clearing the state, locating the next
+ * non-empty stripe column of a pass with a warp ballot, and the dequantising, coalesced
+ * store of the finished block into the subband buffer.  Blocks are pulled from a device
+ * work queue (atomic counter over a host-sorted order, longest blocks first), so CTAs
+ * stay resident and uneven blocks balance out.
+ *
+ * Semantics follow the reference block decoder exactly (decoder/codec/src/
+ * bmi_block_decoder.cpp:10-853, bmi_mq_decoder.h/.cpp, bmi_t1_macro.h): same context-word
+ * layout, same scaled MQ registers and 0xFF/marker handling, same midpoint ("one and a
+ * half") reconstruction bits, same MSB-plane rule including its plane-0 -> plane-1 case for
+ * 9/7 blocks (:708-711), and the same 5/3 placement shift (dec_t1_comp.cpp:341-366).  Raw
+ * (bypass) passes, context reset, per-pass termination and segmentation symbols follow
+ * ITU-T T.800 Annex D (the reference asserts on them).
+ */
+#pragma once
+#include <cstdint>
+
+#include "plan.h"
+
+namespace j2k_dev {
+
+// ---- context-word bits (bmi_t1_macro.h:14-73)
+constexpr uint32_t NBR_ROW0 = 0x1EF;
+constexpr int MU_POS = 20, PI_POS = 21, CHI_POS = 19;
+__device__ __forceinline__ uint32_t ROW_SIG(int k) { return 0x10u << (3 * k); }
+__device__ __forceinline__ uint32_t ROW_CHI(int k) { return 1u << (CHI_POS + 3 * k); }
+__device__ __forceinline__ uint32_t ROW_MU(int k) { return 1u << (MU_POS + 3 * k); }
+__device__ __forceinline__ uint32_t ROW_PI(int k) { return 1u << (PI_POS + 3 * k); }
+__device__ __forceinline__ uint32_t ROW_NBR(int k) { return NBR_ROW0 << (3 * k); }
+constexpr uint32_t MU_ALL = (1u << 20) | (1u << 23) | (1u << 26) | (1u << 29);
+constexpr uint32_t PI_ALL = (1u << 21) | (1u << 24) | (1u << 27) | (1u << 30);
+constexpr uint32_t CHI_ALL = (1u << 19) | (1u << 22) | (1u << 25) | (1u << 28);
+
+enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, N_CTX = 18 };
+
+// Shared tables, filled once per CTA:
+//   mq[94]  : (Qe << 16) | (next state after MPS << 8) | next state after LPS, state = idx*2+mps
+//   zc[3][512]: zero-coding context for LL/LH, HL, HH neighbourhoods
+//   sc[256] : (sign context << 1) | xor bit for an 8-bit (sigma, chi) neighbour index
+struct T1Tables {
+  uint32_t mq[96];
+  uint8_t zc[3][512];
+  uint8_t sc[256];
+};
+
+struct Mq {
+  int32_t A, C;
+  int32_t t, T;
+  uint32_t pos, end;
+  const uint8_t *base;
+};
+
+__device__ __forceinline__ int mq_byte(const Mq &m) { return m.pos < m.end ? (int)__ldg(m.base + m.pos) : 0xFF; }
+
+// FILL_LSBS, bmi_mq_decoder.h:52-73
+__device__ __forceinline__ void mq_fill(Mq &m) {
+  if (m.T == 0xFF) {
+    int b = mq_byte(m);
+    if (b > 0x8F) {
+      m.t = 8;
+    } else {
+      m.T = b << 1;
+      m.pos++;
+      m.t = 7;
+    }
+  } else {
+    m.T = mq_byte(m);
+    m.pos++;
+    m.t = 8;
+  }
+  m.C += m.T;
+}
+
+// Init, bmi_mq_decoder.cpp:186-219 (the 0xFF 0xFF termination is virtual: bytes at or past
+// `end` read as 0xFF)
+__device__ __forceinline__ void mq_init(Mq &m, const uint8_t *base, uint32_t len) {
+  m.base = base;
+  m.pos = 0;
+  m.end = len;
+  m.T = 0;
+  m.C = 0;
+  m.t = 0;
+  mq_fill(m);
+  m.C <<= m.t;
+  mq_fill(m);
+  m.C <<= 7;
+  m.t -= 7;
+  m.A = 0x800000;
+}
+
+// Shift until A >= 0x800000, filling a byte whenever t reaches 0 (the reference's
+// RENORMALIZE_ONCE loop, taken several shifts at a time)
+__device__ __forceinline__ void mq_renorm(Mq &m) {
+  int n = __clz(m.A) - 8;
+  while (n > 0) {
+    if (m.t == 0) mq_fill(m);
+    int k = min(n, m.t);
+    m.A <<= k;
+    m.C <<= k;
+    m.t -= k;
+    n -= k;
+  }
+}
+
+// MQ_DECODE, bmi_mq_decoder.h:86-128
+__device__ __forceinline__ int mq_decode(Mq &m, uint8_t *st, const uint32_t *tab) {
+  uint32_t s = *st;
+  uint32_t e = tab[s];
+  int32_t q = (int32_t)(e >> 16) << 8;
+  int sym = (int)(s & 1);
+  m.A -= q;
+  if (m.C < q) {
+    if (m.A < q) {
+      *st = (uint8_t)(e >> 8);
+    } else {
+      sym ^= 1;
+      *st = (uint8_t)e;
+    }
+    m.A = q;
+    mq_renorm(m);
+  } else {
+    m.C -= q;
+    if (m.A < 0x800000) {
+      if (m.A < q) {
+        sym ^= 1;
+        *st = (uint8_t)e;
+      } else {
+        *st = (uint8_t)(e >> 8);
+      }
+      mq_renorm(m);
+    }
+  }
+  return sym;
+}
+
+// MQ_DECODE_START (fixed Qe 0x5601, MPS 0, no adaptation), bmi_mq_decoder.h:131-169
+__device__ __forceinline__ int mq_uniform(Mq &m) {
+  int ret = 0;
+  if (m.C < 0x560100) {
+    if (m.A >= (0x560100 << 1)) ret = 1;
+    if (!m.t) mq_fill(m);
+    m.C <<= 1;
+    m.t--;
+    m.A = 0x560100 << 1;
+  } else {
+    m.A -= 0x560100;
+    m.C -= 0x560100;
+    if (m.A < 0x800000) {
+      if (m.A < 0x560100) ret = 1;
+      mq_renorm(m);
+    }
+  }
+  return ret;
+}
+
+struct Raw {
+  uint32_t pos, end;
+  const uint8_t *base;
+  uint32_t c;
+  int ct, last;
+};
+__device__ __forceinline__ void raw_init(Raw &r, const uint8_t *base, uint32_t len) {
+  r.base = base;
+  r.pos = 0;
+  r.end = len;
+  r.c = 0;
+  r.ct = 0;
+  r.last = 0;
+}
+// T.800 D.6: after 0xFF the next byte carries 7 bits; bytes past the end read as 0xFF
+__device__ __forceinline__ int raw_bit(Raw &r) {
+  if (r.ct == 0) {
+    int b = r.pos < r.end ? (int)__ldg(r.base + r.pos) : 0xFF;
+    r.pos++;
+    r.ct = (r.last == 0xFF) ? 7 : 8;
+    r.last = b;
+    r.c = (uint32_t)b;
+  }
+  r.ct--;
+  return (int)((r.c >> r.ct) & 1);
+}
+
+// per-warp decode state in shared memory
+struct BlockSmem {
+  uint32_t *cw;  // context words: (stripes + 2) rows of (w + 3) words, + 2
+  int32_t *sp;   // samples: (stripes * 4) x w
+  uint8_t *st;   // 18 MQ context states
+  int w, gap;
+};
+
+__device__ __forceinline__ uint32_t *cword(const BlockSmem &b, int s, int c) {
+  return b.cw + (s + 1) * b.gap + 1 + c;
+}
+
+// sign context index of row k: bit 0 sigma up, 1 chi up, 2 sigma down, 3 chi down,
+// 4 sigma left, 5 chi left, 6 sigma right, 7 chi right
+__device__ __forceinline__ int sign_index(uint32_t cw, uint32_t wl, uint32_t wr, int k) {
+  uint32_t v = cw >> (3 * k);
+  uint32_t chi_up = (k == 0) ? (cw >> 18) & 1 : (v >> 16) & 1;
+  uint32_t idx = ((v >> 1) & 1) | (chi_up << 1) | (((v >> 7) & 1) << 2) | (((v >> 22) & 1) << 3);
+  uint32_t l = wl >> (3 * k), r = wr >> (3 * k);
+  idx |= ((l >> 4) & 1) << 4 | ((l >> 19) & 1) << 5 | ((r >> 4) & 1) << 6 | ((r >> 19) & 1) << 7;
+  return (int)idx;
+}
+
+// Decode (or read raw) the sign of row k, mark the sample significant and spread sigma /
+// chi to the neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).
+template <bool RAW>
+__device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, Mq &mq, Raw &raw,
+                                           const T1Tables &T) {
+  int sym;
+  if (RAW) {
+    sym = raw_bit(raw);
+  } else {
+    int si = sign_index(cw, wp[-1], wp[1], k);
+    int v = T.sc[si];
+    sym = mq_decode(mq, b.st + C_SIGN + (v >> 1), T.mq) ^ (v & 1);
+  }
+  if (k == 0) {
+    uint32_t *up = wp - b.gap;
+    up[-1] |= 0x100u << 9;
+    up[0] |= (0x80u << 9) | ((uint32_t)sym << 31);
+    up[1] |= 0x40u << 9;
+  } else if (k == 3) {
+    uint32_t *dn = wp + b.gap;
+    dn[-1] |= 0x04u;
+    dn[0] |= 0x02u | ((uint32_t)sym << 18);
+    dn[1] |= 0x01u;
+  }
+  wp[-1] |= 0x20u << (3 * k);
+  wp[1] |= 0x08u << (3 * k);
+  cw |= ROW_SIG(k) | ((uint32_t)sym << (CHI_POS + 3 * k));
+  return sym;
+}
+
+// significance propagation (bmi_block_decoder.cpp:10-215)
+template <bool RAW>
+__device__ void pass_sigprop(const BlockSmem &b, int stripes, int p, int band, Mq &mq, Raw &raw, const T1Tables &T,
+                             int lane) {
+  const int32_t one_and_half = (1 << p) + ((1 << p) >> 1);
+  const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
+  for (int s = 0; s < stripes; ++s) {
+    uint32_t *row = cword(b, s, 0);
+    for (int c0 = 0; c0 < b.w; c0 += 32) {
+      // columns with a non-zero word; a sample that becomes significant gives the next
+      // column a significant neighbour, so that column joins the set (columns further
+      // right and the next chunk are unaffected or re-read from memory)
+      __syncwarp();
+      int c = c0 + lane;
+      uint32_t live = __ballot_sync(0xffffffffu, c < b.w && row[c] != 0);
+      while (live) {
+        int bit = __ffs(live) - 1;
+        live &= live - 1;
+        int col = c0 + bit;
+        uint32_t *wp = row + col;
+        uint32_t cw = *wp;
+        bool newsig = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if ((cw & ROW_NBR(k)) && !(cw & (ROW_SIG(k) | ROW_CHI(k)))) {
+            int sym = RAW ? raw_bit(raw) : mq_decode(mq, b.st + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
+            cw |= ROW_PI(k);
+            if (sym) {
+              int sg = decode_sign<RAW>(b, wp, cw, k, mq, raw, T);
+              b.sp[(4 * s + k) * b.w + col] = (int32_t)(((uint32_t)sg << 31) + (uint32_t)one_and_half);
+              newsig = true;
+            }
+          }
+        }
+        *wp = cw;
+        if (newsig && bit < 31 && col + 1 < b.w) live |= 1u << (bit + 1);
+      }
+    }
+  }
+}
+
+// magnitude refinement (bmi_block_decoder.cpp:217-349)
+template <bool RAW>
+__device__ void pass_magref(const BlockSmem &b, int stripes, int p, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
+  const int32_t half = (1 << p) >> 1;
+  for (int s = 0; s < stripes; ++s) {
+    uint32_t *row = cword(b, s, 0);
+    for (int c0 = 0; c0 < b.w; c0 += 32) {
+      __syncwarp();
+      int c = c0 + lane;
+      uint32_t live = __ballot_sync(0xffffffffu, c < b.w && (row[c] & MU_ALL) != 0);
+      while (live) {
+        int bit = __ffs(live) - 1;
+        live &= live - 1;
+        int col = c0 + bit;
+        uint32_t cw = row[col];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          if ((cw & (ROW_MU(k) | ROW_SIG(k))) == (ROW_MU(k) | ROW_SIG(k))) {
+            int32_t *v = &b.sp[(4 * s + k) * b.w + col];
+            int32_t val = *v;
+            int sym;
+            if (RAW) {
+              sym = raw_bit(raw);
+            } else {
+              int ctx = C_MAG;
+              if (((val & 0x7FFFFFFF) >> p) < 4) {
+                if (cw & ROW_NBR(k)) ctx++;
+              } else {
+                ctx += 2;
+              }
+              sym = mq_decode(mq, b.st + ctx, T.mq);
+            }
+            val ^= (int32_t)((uint32_t)(1 - sym) << p);
+            val |= half;
+            *v = val;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// cleanup with run mode (bmi_block_decoder.cpp:351-586)
+__device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, Mq &mq, const T1Tables &T) {
+  const int32_t one_and_half = (1 << p) + ((1 << p) >> 1);
+  const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
+  Raw dummy;
+  for (int s = 0; s < stripes; ++s) {
+    uint32_t *row = cword(b, s, 0);
+    for (int col = 0; col < b.w; ++col) {
+      uint32_t *wp = row + col;
+      uint32_t cw = *wp;
+      int k0 = 0;
+      if (cw == 0) {
+        if (!mq_decode(mq, b.st + C_RUN, T.mq)) continue;  // whole column stays insignificant
+        int r = mq_uniform(mq);
+        r = (r << 1) | mq_uniform(mq);
+        int sg = decode_sign<false>(b, wp, cw, r, mq, dummy, T);
+        b.sp[(4 * s + r) * b.w + col] = (int32_t)(((uint32_t)sg << 31) + (uint32_t)one_and_half);
+        k0 = r + 1;
+      }
+      for (int k = k0; k < 4; ++k) {
+        if (cw & (ROW_SIG(k) | ROW_CHI(k) | ROW_PI(k))) continue;
+        int sym = mq_decode(mq, b.st + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
+        if (sym) {
+          int sg = decode_sign<false>(b, wp, cw, k, mq, dummy, T);
+          b.sp[(4 * s + k) * b.w + col] = (int32_t)(((uint32_t)sg << 31) + (uint32_t)one_and_half);
+        }
+      }
+      cw |= (cw << (MU_POS - 4)) & MU_ALL;
+      cw &= ~PI_ALL;
+      *wp = cw;
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ void init_states(uint8_t *st) {
+  // bmi_mq_decoder.cpp:65-79: (state 0, MPS 0) except sig ctx 0 -> state 4, run -> state 3
+  for (int i = 0; i < N_CTX; ++i) st[i] = 0;
+  st[C_SIG] = 4 << 1;
+  st[C_RUN] = 3 << 1;
+}
+
+__device__ __forceinline__ bool seg_starts(int flags, int j) {
+  if (j == 0) return true;
+  if (flags & J2K_CB_TERMALL) return true;
+  int type = (j - 1) % 3;
+  return (flags & J2K_CB_BYPASS) && j >= 10 && type != 1;
+}
+
+// Decode one code-block with the whole warp.  Returns a status (0 ok).
+template <int MAXW, int MAXH>
+__device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens,
+                            const BlockSmem &b, const T1Tables &T, int lane) {
+  const int w = cb.w, h = cb.h;
+  const int stripes = (h + 3) >> 2;
+  // clear samples and context words; mark OOB columns and a partial last stripe
+  for (int i = lane; i < stripes * 4 * w; i += 32) b.sp[i] = 0;
+  const int nwords = (stripes + 2) * b.gap + 2;
+  for (int i = lane; i < nwords; i += 32) b.cw[i] = 0;
+  __syncwarp();
+  const uint32_t oob = CHI_ALL;
+  for (int s = lane; s < stripes; s += 32) {
+    uint32_t *r = cword(b, s, w);
+    r[0] = oob;
+    r[1] = oob;
+    r[2] = oob;
+  }
+  if (h & 3) {
+    uint32_t m = (h & 3) == 1 ? (ROW_CHI(1) | ROW_CHI(2) | ROW_CHI(3))
+                              : ((h & 3) == 2 ? (ROW_CHI(2) | ROW_CHI(3)) : ROW_CHI(3));
+    for (int c = lane; c < w; c += 32) *cword(b, stripes - 1, c) = m;
+  }
+  if (lane == 0) init_states(b.st);
+  __syncwarp();
+
+  const bool irrev = (cb.flags & J2K_CB_IRREV) != 0;
+  const int missing = cb.missing;
+  const int p_max = 30 - missing;
+  int num_passes = 3 * p_max - 2;
+  if (num_passes > cb.num_passes) num_passes = cb.num_passes;
+  int bit_plane;
+  if (irrev) {
+    bit_plane = (int)cb.mb - 1 - missing;
+  } else {
+    if (((int)cb.mb - missing) * 3 - 2 <= 0) num_passes = 0;
+    bit_plane = -1 - missing;
+  }
+  if (bit_plane < 0) bit_plane = p_max;
+  if (bit_plane == 0) bit_plane = 1;
+  if (num_passes > 0 && p_max <= 0) return 1;
+
+  const int multi = (cb.flags & (J2K_CB_BYPASS | J2K_CB_TERMALL)) != 0;
+  const uint8_t *data = bytes + cb.data_off;
+  Mq mq;
+  Raw raw;
+  mq.A = mq.C = mq.t = mq.T = 0;
+  mq.pos = mq.end = 0;
+  mq.base = data;
+  raw_init(raw, data, 0);
+  uint32_t seg_pos = 0;
+  int seg_idx = 0;
+  bool israw = false;
+  int status = 0;
+  for (int k = 0, type = 2; k < num_passes; ++k, ++type) {
+    if (type == 3) {
+      type = 0;
+      bit_plane--;
+    }
+    if (bit_plane < 0) {
+      status = 2;
+      break;
+    }
+    if (seg_starts(multi ? cb.flags : 0, k)) {
+      uint32_t len;
+      if (multi) {
+        if (seg_idx >= cb.nseg) {
+          status = 3;
+          break;
+        }
+        len = __ldg(seglens + cb.seg_off + seg_idx);
+        seg_idx++;
+      } else {
+        len = cb.data_len;
+      }
+      if (seg_pos + len > cb.data_len) {
+        status = 4;
+        break;
+      }
+      israw = (cb.flags & J2K_CB_BYPASS) && k >= 10 && type != 2;
+      if (israw) raw_init(raw, data + seg_pos, len);
+      else mq_init(mq, data + seg_pos, len);
+      seg_pos += len;
+    }
+    if (type == 0) {
+      if (israw) pass_sigprop<true>(b, stripes, bit_plane, cb.band, mq, raw, T, lane);
+      else pass_sigprop<false>(b, stripes, bit_plane, cb.band, mq, raw, T, lane);
+    } else if (type == 1) {
+      if (israw) pass_magref<true>(b, stripes, bit_plane, mq, raw, T, lane);
+      else pass_magref<false>(b, stripes, bit_plane, mq, raw, T, lane);
+    } else {
+      pass_cleanup(b, stripes, bit_plane, cb.band, mq, T);
+      if (cb.flags & J2K_CB_SEGSYM)
+        for (int i = 0; i < 4; ++i) mq_uniform(mq);
+    }
+    if (cb.flags & J2K_CB_RESET) {
+      __syncwarp();
+      if (lane == 0) init_states(b.st);
+      __syncwarp();
+    }
+  }
+  __syncwarp();
+  return status;
+}
+
+}  // namespace j2k_dev
