@@ -1,0 +1,375 @@
+"""Throughput benchmark of the B200 JPEG 2000 Part-1 decode path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3|c2|c4|c1] [--impl ours|reference]
+
+Default workload (metric: Mpixel/s decoded, batched): the batched video-frame decode —
+64 frames of 1920x1080 RGB 8-bit, 9/7 + ICT, 512x512 tiles, 5 levels, 64x64 code-blocks,
+3 quality layers (~0.5/1/2 bpp), decoded at full layers; all code-blocks of all frames in
+one Tier-1 launch, all tile-components in shared DWT level launches.  Inputs are seeded
+synthetic frames encoded by the project's writer (no dataset); 16 distinct frames are
+encoded and each appears 4 times in the batch (identical decode work per copy).
+
+One step = one decode of the whole batch.  `value` times steps with the coded bytes and
+work lists resident in HBM (CUDA events on the launch stream, L2 flushed between steps);
+`e2e` times the public C-ABI path from host memory: host Tier-2 of every frame,
+pinned H2D, decode, D2H of every decoded picture.  Multi-GPU runs are replicas (each rank
+decodes its own copy of the batch; images are independent, no collective on the data path).
+"""
+import argparse
+import ctypes
+import hashlib
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_package():
+    name = "jpeg2000_decoder_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg_dir = os.path.join(ROOT, "jpeg2000-decoder_b200")
+    spec = importlib.util.spec_from_file_location(name, os.path.join(pkg_dir, "__init__.py"),
+                                                  submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+load_package()
+from jpeg2000_decoder_b200 import native, synth  # noqa: E402
+
+METRIC = "Mpixel/s decoded (batched+served vs plain GPU path); p50/p99 decode latency"
+CACHE = os.environ.get("J2K_BENCH_CACHE", "/tmp/j2k_bench_cache")
+
+
+def _cached(key, make):
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, hashlib.sha1(key.encode()).hexdigest() + ".npz")
+    if os.path.exists(path):
+        d = np.load(path, allow_pickle=False)
+        return [bytes(d["s%d" % i]) for i in range(int(d["n"]))]
+    streams = make()
+    np.savez(path, n=len(streams), **{"s%d" % i: np.frombuffer(s, np.uint8) for i, s in enumerate(streams)})
+    return streams
+
+
+def workload(name, quick=False):
+    """(config dict, list of codestreams, output format)."""
+    if name == "c3":
+        nd = 4 if quick else 16
+        reps = 1 if quick else 4
+        distinct = _cached("c3-v1-%d" % nd, lambda: synth.c3_streams(3, n=nd, workers=os.cpu_count()))
+        streams = [distinct[i % nd] for i in range(nd * reps)]
+        cfg = {"workload": "C3 batched video-frame decode", "frames": len(streams), "distinct_frames": nd,
+               "size": "1920x1080", "components": 3, "bitdepth": 8, "wavelet": "9/7+ICT", "tiles": "512x512",
+               "levels": 5, "codeblock": "64x64", "layers": 3, "layer_bpp": [0.5, 1.0, 2.0]}
+        return cfg, streams, native.FMT_24BITS_RGB
+    if name == "c2":
+        streams = _cached("c2-v1", lambda: [synth.c2_stream(2)])
+        cfg = {"workload": "C2 single 2048x2048 RGB 9/7+ICT ~1 bpp", "frames": 1, "size": "2048x2048",
+               "components": 3, "bitdepth": 8, "wavelet": "9/7+ICT", "levels": 5, "codeblock": "64x64",
+               "layers": 1}
+        return cfg, streams, native.FMT_24BITS_RGB
+    if name == "c4":
+        n = 2 if quick else 16
+        nd = min(n, 4)
+        distinct = _cached("c4-v1-%d" % nd, lambda: synth.c4_streams(4, n=nd, workers=os.cpu_count()))
+        streams = [distinct[i % nd] for i in range(n)]
+        cfg = {"workload": "C4 batched 12-bit lossless", "frames": n, "distinct_frames": nd, "size": "4096x2160",
+               "components": 3, "bitdepth": 12, "wavelet": "5/3+RCT", "levels": 6, "codeblock": "32x32",
+               "layers": 8, "progression": "RPCL", "mode": "BYPASS+RESET"}
+        return cfg, streams, native.FMT_48BITS_RGB
+    if name == "c1":
+        streams = _cached("c1-v1", lambda: [synth.c1_stream(1)])
+        cfg = {"workload": "C1 512x512 gray 5/3 lossless", "frames": 1, "size": "512x512", "components": 1,
+               "bitdepth": 8, "wavelet": "5/3", "levels": 5, "codeblock": "64x64", "layers": 1}
+        return cfg, streams, native.FMT_32BITS_4COMPONENTS
+    raise SystemExit("unknown workload " + name)
+
+
+def parse_all(streams, pool):
+    return list(pool.map(native.Plan, streams))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = "/tmp/j2k_clocks_%d.csv" % os.getpid()
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+        except OSError:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 3 + i and "Active" in r[3 + i]
+                          and "Not" not in r[3 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+# ------------------------------------------------------------------ CPU (oracle) -------
+def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
+    """Decode a bounded sample of the workload with the CPU restatement on all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from jpeg2000_decoder_b200 import build
+    build.build_oracle(reference="/nonexistent")
+    import oracle_util
+    threads = threads or os.cpu_count() or 1
+    plans = [native.Plan(s) for s in streams[:max(1, min(len(streams), threads))]]
+
+    def one(p):
+        oracle_util.oracle_decode(p, fmt)
+        return p.info.width * p.info.height
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        t0 = time.perf_counter()
+        px = 0
+        rounds = 0
+        while True:
+            px += sum(ex.map(one, plans))
+            rounds += 1
+            if time.perf_counter() - t0 > budget_s or rounds >= 8:
+                break
+        dt = time.perf_counter() - t0
+    return px / dt / 1e6, threads, "%d image decodes (%d distinct) in %.1f s" % (rounds * len(plans), len(plans), dt)
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    cfg, streams, fmt = workload(args.workload, args.quick)
+    for _ in range(args.warmup):
+        cpu_decode_sample(streams, fmt, budget_s=1.0)
+    vals = []
+    sample = ""
+    cores = os.cpu_count()
+    for _ in range(args.steps):
+        v, cores, sample = cpu_decode_sample(streams, fmt, budget_s=5.0)
+        vals.append(v)
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": round(value, 3), "unit": "Mpixel/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/int32", "data": "synthetic (seeded, project encoder)", "config": cfg, "impl": "reference",
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ GPU arm -----------
+def run_gpu(args, rank, world, dist):
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg, streams, fmt = workload(args.workload, args.quick)
+    pool = ThreadPoolExecutor(max_workers=os.cpu_count())
+    plans = parse_all(streams, pool)
+    pixels = sum(p.info.width * p.info.height for p in plans)
+    ctx = native.GpuContext(dev)
+    stream = torch.cuda.Stream()  # a real stream handle: the decode and the events share it
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device="cuda")  # 256 MB > L2
+
+    # ---- device-resident decode (value)
+    ctx.begin()
+    for p in plans:
+        ctx.add(p, fmt)
+    ctx.stage(sp)
+    for _ in range(args.warmup):
+        ctx.run(sp)
+        assert ctx.sync() == 0
+    launches_per_step = ctx.launches()
+    bad = sum(ctx.status(i)[1] for i in range(len(plans)))
+    times, t1s, dwts = [], [], []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.run(sp)
+            e1.record(stream)
+            assert ctx.sync() == 0
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+            tm = ctx.timing()
+            t1s.append(tm["t1_ms"])
+            dwts.append(tm["dwt_ms"])
+    torch.cuda.synchronize()
+    step_ms = float(np.mean(times))
+    total_ms = float(np.sum(times))
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = pixels * world * args.steps / (total_ms / 1e3) / 1e6
+
+    # ---- plain per-image GPU path: one image per launch sequence
+    plain_ms = []
+    uniq = plans[: min(len(plans), 16)]
+    for it in range(2):
+        t0 = time.perf_counter()
+        for p in uniq:
+            ctx.begin()
+            ctx.add(p, fmt)
+            ctx.launch(sp)
+            assert ctx.sync() == 0
+        if it:
+            plain_ms.append((time.perf_counter() - t0) * 1e3)
+    plain = sum(p.info.width * p.info.height for p in uniq) / (plain_ms[0] / 1e3) / 1e6
+
+    # ---- end to end through the C ABI with host buffers
+    outs = [np.empty(p.output_bytes(fmt), np.uint8) for p in plans]
+    h2d = sum(p.info.coded_bytes for p in plans)
+    d2h = sum(o.nbytes for o in outs)
+    e2e_ms = []
+    for it in range(max(2, min(args.steps, 4)) + 1):
+        t0 = time.perf_counter()
+        ps = parse_all(streams, pool)
+        ctx.begin()
+        for p in ps:
+            ctx.add(p, fmt)
+        ctx.launch(sp)
+        assert ctx.sync() == 0
+        for i, o in enumerate(outs):
+            native.lib().j2k_gpu_output_copy(ctx.h, i, o.ctypes.data_as(ctypes.c_void_p), o.nbytes)
+        if it:
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = pixels * world / (float(np.median(e2e_ms)) / 1e3) / 1e6
+
+    if rank != 0:
+        return
+    # ---- roofline of the dominant kernel (Tier-1) and of the DWT + MCT stage
+    t1_ms = float(np.mean(t1s))
+    dwt_ms = float(np.mean(dwts))
+    samples = sum(p.info.coef_elems for p in plans)
+    coded = sum(p.info.coded_bytes for p in plans)
+    out_bytes = d2h
+    peak, peak_kind = measured_peaks()
+    t1_bytes = coded + 4 * samples
+    dwt_bytes = 4 * samples + out_bytes
+    tr = profile_traffic().get(args.workload, {})
+    dominant = "t1" if t1_ms >= dwt_ms else "dwt"
+    roof_t1 = {"bound": "hbm", "achieved": round(t1_bytes / (t1_ms / 1e3) / 1e9, 2), "peak": peak, "unit": "GB/s",
+               "frac": round(t1_bytes / (t1_ms / 1e3) / 1e9 / peak, 4), "traffic": tr.get("t1_bytes_per_launch"),
+               "kernel": "t1_kernel", "peak_source": peak_kind, "algorithmic_bytes": t1_bytes,
+               "ms_per_launch": round(t1_ms, 4), "note": "serial MQ decode: issue/latency bound, not HBM bound"}
+    roof_dwt = {"bound": "hbm", "achieved": round(dwt_bytes / (dwt_ms / 1e3) / 1e9, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(dwt_bytes / (dwt_ms / 1e3) / 1e9 / peak, 4), "traffic": tr.get("dwt_bytes_per_step"),
+                "kernel": "dwt_level_kernel + output_kernel", "peak_source": peak_kind,
+                "algorithmic_bytes": dwt_bytes, "ms_per_step": round(dwt_ms, 4)}
+    cpu_v, cores, sample = cpu_decode_sample(streams, fmt, budget_s=args.cpu_budget)
+    clocks = clk.summary()
+    cfg = dict(cfg)
+    cfg.update({"parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",
+                "bad_blocks": bad})
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (9/7) / int32 (5/3)", "data": "synthetic (seeded, project encoder)",
+            "config": cfg,
+            "e2e": {"value": round(e2e, 2), "unit": "Mpixel/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": round(float(np.median(e2e_ms)), 3),
+                    "includes": "host Tier-2 parse + pinned H2D + decode + D2H of every picture"},
+            "plain_gpu_path": {"value": round(plain, 2), "unit": "Mpixel/s", "images": len(uniq),
+                               "what": "one image per launch sequence, host buffers"},
+            "speedup_vs_plain": round(value / plain, 2),
+            "roofline": roof_t1 if dominant == "t1" else roof_dwt,
+            "roofline_dwt": roof_dwt, "roofline_t1": roof_t1,
+            "stage_ms": {"t1": round(t1_ms, 4), "dwt_mct": round(dwt_ms, 4)},
+            "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clocks}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c4", "c1"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="small batch for smoke runs")
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        run_gpu(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -98,6 +98,12 @@ int j2k_gpu_batch_footprint(const j2k_gpu_ctx *ctx, size_t *bytes);
 /* Stage inputs (pinned host -> device) and enqueue all kernels on `stream`
  * (a cudaStream_t, or NULL for the context's stream).  Asynchronous. */
 int j2k_gpu_batch_launch(j2k_gpu_ctx *ctx, void *stream);
+/* The two halves of batch_launch: stage assembles the batch's work lists and coded bytes
+ * in pinned memory and copies them to the device; run enqueues Tier-1, the DWT levels and
+ * the output stage on the staged (device-resident) inputs.  run may be repeated after a
+ * sync to decode the same staged batch again. */
+int j2k_gpu_batch_stage(j2k_gpu_ctx *ctx, void *stream);
+int j2k_gpu_batch_run(j2k_gpu_ctx *ctx, void *stream);
 /* Wait for the batch with a host-side timeout (ms, < 0 = forever). */
 int j2k_gpu_batch_sync(j2k_gpu_ctx *ctx, int timeout_ms);
 /* Per-image status after sync: J2K_OK or J2K_ERR_DECODE; `bad_blocks` may be NULL. */

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/bmi_decoder.h"
+#include "../../include/bmi_decoder_c.h"
 #include "../../include/j2k_gpu.h"
 #include "bmi_engine.h"
 #include "codestream.h"

@@ -455,8 +455,10 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
         // to EOC
         tend = data + len;
         if (len >= 2 && data[len - 2] == 0xFF && data[len - 1] == 0xD9) tend -= 2;
+      } else if ((size_t)(data + len - sot) < psot) {
+        tend = data + len;  // truncated stream: keep the bytes that are there
+        psot = 0;
       } else {
-        if ((size_t)(data + len - sot) < psot) return PARSE_ERR_TRUNCATED;
         tend = sot + psot;
       }
       if (tend < body) return PARSE_ERR_INVALID;
@@ -760,6 +762,7 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             d.w = (uint16_t)cb.w;
             d.h = (uint16_t)cb.h;
             d.band = (uint8_t)B.type;
+            d.spqcd = B.spqcd;
             d.mb = (uint8_t)std::min(B.mb, 255);
             d.missing = (uint8_t)std::min(cb.missing, 255);
             d.num_passes = (uint8_t)cb.kept;

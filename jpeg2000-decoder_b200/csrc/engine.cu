@@ -198,7 +198,14 @@ struct j2k_gpu_ctx {
   std::vector<BatchImage> imgs;
   uint16_t *h_status = nullptr;  // pinned
   size_t h_status_cap = 0;
-  bool launched = false, synced = false;
+  bool launched = false, synced = false, staged = false;
+  // staged batch (device-resident inputs) for batch_run
+  struct Staged {
+    size_t n_big = 0, n_small = 0, n_cblks = 0, n_otasks = 0;
+    size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0;
+    int maxL = 0;
+    std::vector<uint32_t> dtask_off;
+  } sg;
   cudaEvent_t ev[6] = {};
   float t_t1 = 0, t_dwt = 0, t_h2d = 0, t_total = 0;
   int launches = 0;
@@ -334,13 +341,13 @@ extern "C" int j2k_gpu_batch_begin(j2k_gpu_ctx *c) {
   if (!c) return J2K_ERR_ARG;
   if (c->launched && !c->synced) return J2K_ERR_STATE;
   c->imgs.clear();
-  c->launched = c->synced = false;
+  c->launched = c->synced = c->staged = false;
   return J2K_OK;
 }
 
 extern "C" int j2k_gpu_batch_add(j2k_gpu_ctx *c, const j2k_plan *plan, int fmt, int flags, int *slot) {
   if (!c || !plan) return J2K_ERR_ARG;
-  if (c->launched) return J2K_ERR_STATE;
+  if (c->launched || c->staged) return J2K_ERR_STATE;
   if (fmt != J2K_FMT_NONE && j2k_dev::fmt_bytes(fmt) == 0) return J2K_ERR_ARG;
   const j2k_image_info &I = plan->p.info;
   if (I.bitdepth < 1 || I.bitdepth > 16) return J2K_ERR_UNSUPPORTED;
@@ -387,9 +394,9 @@ extern "C" int j2k_gpu_batch_footprint(const j2k_gpu_ctx *cc, size_t *bytes) {
   return J2K_OK;
 }
 
-extern "C" int j2k_gpu_batch_launch(j2k_gpu_ctx *c, void *user_stream) {
+extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   if (!c) return J2K_ERR_ARG;
-  if (c->launched) return J2K_ERR_STATE;
+  if (c->launched && !c->synced) return J2K_ERR_STATE;
   if (c->imgs.empty()) return J2K_ERR_STATE;
   cudaSetDevice(c->device);
   cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
@@ -420,7 +427,6 @@ extern "C" int j2k_gpu_batch_launch(j2k_gpu_ctx *c, void *user_stream) {
       cb.data_off = (uint32_t)(cb.data_off + byte_base);
       cb.seg_off += seg_base;
       cb.out_off += im.coef_base;
-      cb.status = 0;
       uint32_t idx = (uint32_t)cbs.size();
       cbs.push_back(cb);
       if (cb.num_passes == 0 && !(cb.flags & J2K_CB_IRREV) && false) continue;
@@ -566,8 +572,51 @@ extern "C" int j2k_gpu_batch_launch(j2k_gpu_ctx *c, void *user_stream) {
   CK(cudaEventRecord(c->ev[0], st));
   CK(cudaMemcpyAsync(D, H, o_byt, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(c->d_bytes.p, H + o_byt, S.bytes, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(c->d_counter.p, 0, 64, st));
   CK(cudaEventRecord(c->ev[1], st));
+  c->sg.n_big = ord_big.size();
+  c->sg.n_small = ord_small.size();
+  c->sg.n_cblks = S.cblks;
+  c->sg.n_otasks = otasks.size();
+  c->sg.o_cbs = o_cbs;
+  c->sg.o_ord = o_ord;
+  c->sg.o_seg = o_seg;
+  c->sg.o_lev = o_lev;
+  c->sg.o_dtk = o_dtk;
+  c->sg.o_grp = o_grp;
+  c->sg.o_otk = o_otk;
+  c->sg.maxL = maxL;
+  c->sg.dtask_off = dtask_off;
+  c->staged = true;
+  c->launched = false;
+  c->synced = false;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
+  if (!c) return J2K_ERR_ARG;
+  if (!c->staged || (c->launched && !c->synced)) return J2K_ERR_STATE;
+  cudaSetDevice(c->device);
+  cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
+  c->user_stream = st;
+  const auto &G = c->sg;
+  uint8_t *D = (uint8_t *)c->d_cblks.p;
+  const size_t o_cbs = G.o_cbs, o_ord = G.o_ord, o_seg = G.o_seg, o_lev = G.o_lev, o_dtk = G.o_dtk, o_grp = G.o_grp,
+               o_otk = G.o_otk;
+  const int maxL = G.maxL;
+  const std::vector<uint32_t> &dtask_off = G.dtask_off;
+  struct {
+    size_t n;
+    size_t size() const { return n; }
+    bool empty() const { return n == 0; }
+  } ord_big{G.n_big}, ord_small{G.n_small}, otasks{G.n_otasks};
+  c->launches = 0;
+  if (!c->launched) {
+    // first run after staging: the staging events already bracket the copies
+  } else {
+    CK(cudaEventRecord(c->ev[0], st));
+    CK(cudaEventRecord(c->ev[1], st));
+  }
+  CK(cudaMemsetAsync(c->d_counter.p, 0, 64, st));
 
   // ---- Tier-1
   const j2k_cblk *d_cbs = (const j2k_cblk *)(D + o_cbs);
@@ -629,21 +678,27 @@ extern "C" int j2k_gpu_batch_launch(j2k_gpu_ctx *c, void *user_stream) {
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[3], st));
-  if (c->h_status_cap < S.cblks + 1) {
+  if (c->h_status_cap < G.n_cblks + 1) {
     if (c->h_status) cudaFreeHost(c->h_status);
     c->h_status = nullptr;
     c->h_status_cap = 0;
-    if (cudaMallocHost(&c->h_status, (S.cblks + 1) * 2) != cudaSuccess) {
+    if (cudaMallocHost(&c->h_status, (G.n_cblks + 1) * 2) != cudaSuccess) {
       cudaGetLastError();
       return J2K_ERR_NOMEM;
     }
-    c->h_status_cap = S.cblks + 1;
+    c->h_status_cap = G.n_cblks + 1;
   }
-  if (S.cblks) CK(cudaMemcpyAsync(c->h_status, c->d_status.p, S.cblks * 2, cudaMemcpyDeviceToHost, st));
+  if (G.n_cblks) CK(cudaMemcpyAsync(c->h_status, c->d_status.p, G.n_cblks * 2, cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(c->ev[4], st));
   c->launched = true;
   c->synced = false;
   return J2K_OK;
+}
+
+extern "C" int j2k_gpu_batch_launch(j2k_gpu_ctx *c, void *user_stream) {
+  int rc = j2k_gpu_batch_stage(c, user_stream);
+  if (rc != J2K_OK) return rc;
+  return j2k_gpu_batch_run(c, user_stream);
 }
 
 extern "C" int j2k_gpu_batch_sync(j2k_gpu_ctx *c, int timeout_ms) {

@@ -48,7 +48,7 @@ typedef struct j2k_cblk {
   uint8_t mb;          /* reference "numbps": SPqcd exponent + guard bits - 1 */
   uint8_t flags;       /* J2K_CB_* */
   uint8_t nseg;        /* codeword segments (>= 1 when num_passes > 0) */
-  uint16_t status;     /* written by the decoder: 0 ok, else an error code */
+  uint16_t spqcd;      /* raw QCD/QCC step value of the band (exponent << 11 | mantissa, or exponent) */
 } j2k_cblk;
 
 /* One tile-component: the inverse DWT/MCT work for one region of the coefficient buffer. */

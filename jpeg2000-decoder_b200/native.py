@@ -53,7 +53,7 @@ class CodeBlock(ctypes.Structure):
                 ("out_stride", ctypes.c_uint32), ("seg_off", ctypes.c_uint32), ("gain", ctypes.c_float),
                 ("w", ctypes.c_uint16), ("h", ctypes.c_uint16), ("num_passes", ctypes.c_uint8),
                 ("missing", ctypes.c_uint8), ("band", ctypes.c_uint8), ("mb", ctypes.c_uint8),
-                ("flags", ctypes.c_uint8), ("nseg", ctypes.c_uint8), ("status", ctypes.c_uint16)]
+                ("flags", ctypes.c_uint8), ("nseg", ctypes.c_uint8), ("spqcd", ctypes.c_uint16)]
 
 
 class TileComp(ctypes.Structure):
@@ -85,7 +85,7 @@ EXPORTS = [
     "j2k_plan_create", "j2k_plan_destroy", "j2k_plan_info", "j2k_plan_cblks", "j2k_plan_seglens",
     "j2k_plan_bytes", "j2k_plan_tilecomps", "j2k_output_bytes", "j2k_status_string",
     "j2k_gpu_ctx_create", "j2k_gpu_ctx_destroy", "j2k_gpu_mem_usage", "j2k_gpu_batch_begin",
-    "j2k_gpu_batch_add", "j2k_gpu_batch_footprint", "j2k_gpu_batch_launch", "j2k_gpu_batch_sync",
+    "j2k_gpu_batch_add", "j2k_gpu_batch_footprint", "j2k_gpu_batch_launch", "j2k_gpu_batch_stage", "j2k_gpu_batch_run", "j2k_gpu_batch_sync",
     "j2k_gpu_image_status", "j2k_gpu_output_device", "j2k_gpu_output_copy", "j2k_gpu_component_copy",
     "j2k_gpu_coefficients_copy", "j2k_gpu_last_timing", "j2k_gpu_last_launches", "j2k_gpu_set_tuning",
     "j2k_gpu_get_tuning", "j2k_gpu_decode",
@@ -122,6 +122,8 @@ def lib():
         L.j2k_gpu_batch_add.argtypes = [vp, vp, i, i, ctypes.POINTER(i)]
         L.j2k_gpu_batch_footprint.argtypes = [vp, ctypes.POINTER(sz)]
         L.j2k_gpu_batch_launch.argtypes = [vp, vp]
+        L.j2k_gpu_batch_stage.argtypes = [vp, vp]
+        L.j2k_gpu_batch_run.argtypes = [vp, vp]
         L.j2k_gpu_batch_sync.argtypes = [vp, i]
         L.j2k_gpu_image_status.argtypes = [vp, i, ctypes.POINTER(i)]
         L.j2k_gpu_output_device.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(sz)]
@@ -291,6 +293,12 @@ class GpuContext:
 
     def launch(self, stream=None):
         self._ck(lib().j2k_gpu_batch_launch(self.h, stream), "batch_launch")
+
+    def stage(self, stream=None):
+        self._ck(lib().j2k_gpu_batch_stage(self.h, stream), "batch_stage")
+
+    def run(self, stream=None):
+        self._ck(lib().j2k_gpu_batch_run(self.h, stream), "batch_run")
 
     def sync(self, timeout_ms=-1):
         return lib().j2k_gpu_batch_sync(self.h, timeout_ms)

@@ -1,0 +1,253 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the oracle.
+
+Bar: bit-exact for Tier-1 coefficients, 5/3 and RCT; for 9/7 + ICT the FP32 path uses the
+reference's operation order and is expected bit-exact as well (tolerance: 0 LSB), with
+PSNR / max-abs against an FP64 synthesis reported.  At full benchmark sizes the check is
+a size-independent property (lossless identity, or a batch decoded alone equals the same
+image decoded inside a mixed batch)."""
+import ctypes
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_util
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _read(name):
+    with open(os.path.join(GOLDEN, name), "rb") as f:
+        return f.read()
+
+
+def _decode_check(ctx, cs, fmt, flags=0):
+    """GPU decode of one stream; compares Tier-1 coefficients and output with the oracle."""
+    from jpeg2000_decoder_b200 import native
+    out, rc, bad, plan = ctx.decode(cs, fmt, flags)
+    assert rc == native.J2K_OK and bad == 0
+    t1 = ctx.coefficients(0, 0).view(np.int32)
+    obad, ot1 = oracle_util.oracle_t1_coefficients(plan)
+    assert obad == 0
+    assert np.array_equal(t1, ot1), "Tier-1 coefficients differ from the oracle"
+    orc, oout, _ = oracle_util.oracle_decode(plan, fmt, ref_compat=1 if flags & native.FLAG_REF_COMPAT else 0)
+    if fmt != native.FMT_NONE:
+        assert np.array_equal(out, oout), "decoded picture differs from the oracle (max |d| = %d)" % int(
+            np.abs(out.astype(int) - oout.astype(int)).max())
+    return out, plan
+
+
+@pytest.mark.parametrize("name", sorted(n for n in os.listdir(GOLDEN) if n.endswith(".j2k")))
+@pytest.mark.parametrize("flags", [0, 1])
+def test_golden_streams_bit_exact(gpu_ctx, name, flags):
+    from jpeg2000_decoder_b200 import native
+    cs = _read(name)
+    plan = native.Plan(cs)
+    fmt = native.FMT_32BITS_4COMPONENTS if plan.info.ncomp == 1 else (
+        native.FMT_48BITS_RGB if plan.info.bitdepth > 8 else native.FMT_24BITS_RGB)
+    _decode_check(gpu_ctx, cs, fmt, flags)
+
+
+def test_golden_t1_against_reference_digests(gpu_ctx):
+    """GPU Tier-1 of each block hashed exactly as the reference's decode_code_block output."""
+    from jpeg2000_decoder_b200 import native
+    golden = json.load(open(os.path.join(GOLDEN, "golden.json")))
+    for name, g in golden.items():
+        if "reference_t1_sha256_16" not in g:
+            continue
+        plan = native.Plan(_read(name))
+        gpu_ctx.begin()
+        gpu_ctx.add(plan, native.FMT_NONE)
+        gpu_ctx.launch()
+        assert gpu_ctx.sync() == 0
+        coef = gpu_ctx.coefficients(0, 0).view(np.int32)
+        # re-derive each block's raw output from the GPU coefficients is not possible for
+        # 9/7 (dequantised floats), so compare GPU placement against the oracle placement of
+        # the reference-pinned raw samples
+        _, ot1 = oracle_util.oracle_t1_coefficients(plan)
+        assert np.array_equal(coef, ot1), name
+        for i, want in enumerate(g["reference_t1_sha256_16"][:8]):
+            rc, raw = oracle_util.oracle_block(plan, i)
+            assert hashlib.sha256(raw.tobytes()).hexdigest()[:16] == want
+
+
+def test_c1_lossless_and_reference_rows(gpu_ctx):
+    from jpeg2000_decoder_b200 import native, synth
+    src = synth.sinusoid_gray(1)[0]
+    cs = synth.c1_stream(1)
+    out, _ = _decode_check(gpu_ctx, cs, native.FMT_32BITS_4COMPONENTS, 0)
+    assert np.array_equal(out.reshape(512, 512, 4)[:, :, 3], src)
+    out, _ = _decode_check(gpu_ctx, cs, native.FMT_32BITS_4COMPONENTS, native.FLAG_REF_COMPAT)
+    bad = np.nonzero((out.reshape(512, 512, 4)[:, :, 3] != src).any(axis=1))[0]
+    assert len(bad) == 31 and bad.min() == 481
+
+
+def test_c2_97_ict_1bpp_exact_and_fp64_budget(gpu_ctx):
+    """C2 at full size: 2048x2048 RGB, 9/7 + ICT at ~1 bpp."""
+    from jpeg2000_decoder_b200 import native, synth
+    cs = synth.c2_stream(2)
+    assert abs(len(cs) * 8 / (2048 * 2048) - 1.0) < 0.05
+    out, plan = _decode_check(gpu_ctx, cs, native.FMT_24BITS_RGB)
+    rgb = out.reshape(2048, 2048, 3)[:, :, ::-1].transpose(2, 0, 1)
+    psnr, maxabs = oracle_util.psnr_maxabs(rgb, oracle_util.fp64_decode(plan), 8)
+    print("C2 vs FP64 9/7: PSNR %.2f dB, max-abs %.1f" % (psnr, maxabs))
+    assert psnr > 45
+
+
+def test_c3_frames_tiles_layers(gpu_ctx):
+    """C3 shape (1920x1080, 512x512 tiles, 3 layers) on 3 frames, each exact vs the oracle."""
+    from jpeg2000_decoder_b200 import native, synth
+    frames = synth.video_frames(3, n=3)
+    for f in frames:
+        cs = native.encode(f, 8, **synth.C3_PARAMS)
+        _decode_check(gpu_ctx, cs, native.FMT_24BITS_RGB)
+
+
+def test_c4_bypass_reset_lossless_full_size(gpu_ctx):
+    """C4 at full size (4096x2160 RGB 12-bit, 5/3 + RCT, BYPASS + RESET, 8 layers, RPCL):
+    decoded samples equal the source exactly; the reduced-size copy also equals the oracle."""
+    from jpeg2000_decoder_b200 import native, synth
+    img = synth.fractal_rgb(4000, 2160, 4096)
+    cs = native.encode(img, 12, **synth.C4_PARAMS)
+    out, rc, bad, plan = gpu_ctx.decode(cs, native.FMT_48BITS_RGB)
+    assert rc == 0 and bad == 0
+    rgb = out.view(np.uint16).reshape(2160, 4096, 3)[:, :, ::-1].transpose(2, 0, 1) >> 4
+    assert np.array_equal(rgb, img)
+    small = native.encode(img[:, :270, :512], 12, **synth.C4_PARAMS)
+    _decode_check(gpu_ctx, small, native.FMT_48BITS_RGB)
+
+
+def test_batch_alone_equals_mixed(gpu_ctx):
+    """Each image of a mixed batch (sizes, wavelets, bit depths) equals its solo decode."""
+    from jpeg2000_decoder_b200 import native, synth
+    streams = [synth.c5_request(s)[0] for s in range(6)] + [_read("c1_gray_53.j2k"), _read("rgb256_97_1bpp.j2k")]
+    fmts = []
+    solo = []
+    for cs in streams:
+        plan = native.Plan(cs)
+        fmt = native.FMT_32BITS_4COMPONENTS if plan.info.ncomp == 1 else (
+            native.FMT_48BITS_RGB if plan.info.bitdepth > 8 else native.FMT_24BITS_RGB)
+        fmts.append(fmt)
+        out, rc, bad, _ = gpu_ctx.decode(cs, fmt)
+        assert rc == 0
+        solo.append(out)
+    plans = [native.Plan(cs) for cs in streams]
+    gpu_ctx.begin()
+    slots = [gpu_ctx.add(p, f) for p, f in zip(plans, fmts)]
+    gpu_ctx.launch()
+    assert gpu_ctx.sync() == 0
+    for s, want in zip(slots, solo):
+        assert gpu_ctx.status(s)[0] == 0
+        assert np.array_equal(gpu_ctx.output(s), want)
+
+
+def test_components_and_reduced_resolution(gpu_ctx):
+    from jpeg2000_decoder_b200 import native
+    cs = _read("rgb300x200_97_tiles_3layers.j2k")
+    plan = native.Plan(cs)
+    gpu_ctx.begin()
+    gpu_ctx.add(plan, native.FMT_NONE)
+    gpu_ctx.launch()
+    assert gpu_ctx.sync() == 0
+    comp = gpu_ctx.component(0, 1)
+    assert comp.shape == (200, 300) and comp.dtype == np.float32
+    # reduced resolution: discard 2 levels
+    small = native.Plan(cs, discard_levels=2)
+    gpu_ctx.begin()
+    gpu_ctx.add(small, native.FMT_24BITS_RGB)
+    gpu_ctx.launch()
+    assert gpu_ctx.sync() == 0
+    out = gpu_ctx.output(0)
+    orc, oout, _ = oracle_util.oracle_decode(small, native.FMT_24BITS_RGB)
+    assert out.size == 75 * 50 * 3 and np.array_equal(out, oout)
+
+
+def test_bmi_decoder_api(pkg):
+    """The reference-facing BMI::Decoder through its C binding."""
+    from jpeg2000_decoder_b200 import native, synth
+    L = native.lib()
+    assert L.bmi_decoder_init(1, 2) == 0
+    L.bmi_decoder_set_job(native.FMT_32BITS_4COMPONENTS, -1, 0, -1)
+    cs = _read("c1_gray_53.j2k")
+    ms = ctypes.c_double()
+    h1 = L.bmi_decoder_decode(cs, len(cs), ctypes.byref(ms))
+    assert L.bmi_decoder_status(h1) == 0  # READY
+    n = ctypes.c_int()
+    p = L.bmi_decoder_result(h1, ctypes.byref(n))
+    assert n.value == 512 * 512 * 4
+    gray = np.frombuffer(ctypes.string_at(p, n.value), np.uint8).reshape(512, 512, 4)[:, :, 3]
+    assert np.array_equal(gray, synth.sinusoid_gray(1)[0])
+    ci = L.bmi_decoder_component_int(h1, 0, ctypes.byref(n))
+    comp = np.frombuffer(ctypes.string_at(ci, n.value), np.int32).reshape(512, 512)
+    assert np.array_equal(comp + 128, synth.sinusoid_gray(1)[0].astype(np.int32))
+    t = L.bmi_decoder_thumbnail(h1, ctypes.byref(n))
+    assert t and n.value == 16 * 16 * 4
+    # the output ring holds 2 pictures: the first handler is released by the third decode
+    h2 = L.bmi_decoder_decode(cs, len(cs), None)
+    h3 = L.bmi_decoder_decode(cs, len(cs), None)
+    assert h3 > h2 > h1
+    assert L.bmi_decoder_status(h1) == 11  # RELEASED
+    assert L.bmi_decoder_status(h3) == 0
+    L.bmi_decoder_release(h3)
+    assert L.bmi_decoder_decode(b"junk", 4, None) > 0
+    L.bmi_decoder_terminate()
+
+
+def test_bmi_dec_c_api(pkg):
+    """BMI_dec_info / BMI_dec_init / BMI_dec / BMI_dec_thumbnail / BMI_dec_exit."""
+    from jpeg2000_decoder_b200 import native, synth
+
+    class DecParam(ctypes.Structure):
+        _fields_ = [("mempool", ctypes.c_void_p * 2), ("pool_size", ctypes.c_int * 2), ("input", ctypes.c_void_p),
+                    ("output", ctypes.c_void_p * 4), ("in_size", ctypes.c_uint)] + \
+                   [(n, ctypes.c_int) for n in ("width", "height", "bitdepth", "format", "num_components", "cb_width",
+                                                "cb_height", "prec_width", "prec_height", "tile_width", "tile_height",
+                                                "tile_num", "size_opt", "layer", "dwt_level", "roi_shift",
+                                                "progression", "configuration", "guard_bit")] + \
+                   [("quant_step", ctypes.c_uint * 31)]
+    L = native.lib()
+    cs = _read("rgb256_53_rct.j2k")
+    buf = ctypes.create_string_buffer(cs, len(cs))
+    p = DecParam()
+    p.input = ctypes.cast(buf, ctypes.c_void_p)
+    p.in_size = len(cs)
+    assert L.BMI_dec_info(ctypes.byref(p), 1) == 0
+    assert (p.width, p.height, p.num_components, p.bitdepth, p.dwt_level) == (256, 256, 3, 8, 5)
+    assert L.BMI_dec_init(ctypes.byref(p), 1, 1) == -1  # pools missing
+    pools = [ctypes.create_string_buffer(max(1, p.pool_size[k])) for k in range(2)]
+    p.mempool[0] = ctypes.cast(pools[0], ctypes.c_void_p)
+    p.mempool[1] = ctypes.cast(pools[1], ctypes.c_void_p)
+    assert L.BMI_dec_init(ctypes.byref(p), 1, 1) == 0
+    planes = [np.zeros((256, 256), np.uint8) for _ in range(3)]
+    outs = (ctypes.c_void_p * 4)(*[pl.ctypes.data for pl in planes], None)
+    assert L.BMI_dec(ctypes.byref(p), outs, 1) == 0
+    assert np.array_equal(np.stack(planes), synth.fields_and_edges(11, 256, 256))
+    thumbs = [np.zeros((64, 64), np.uint8) for _ in range(3)]
+    touts = (ctypes.c_void_p * 4)(*[pl.ctypes.data for pl in thumbs], None)
+    assert L.BMI_dec_thumbnail(ctypes.byref(p), touts, 2, 1) == 1  # PARSING = success
+    assert L.BMI_dec_exit(ctypes.byref(p)) == 0
+
+
+def test_corrupt_blocks_do_not_hang(gpu_ctx):
+    """Corrupted packet bodies decode to completion within the host timeout."""
+    from jpeg2000_decoder_b200 import native
+    cs = bytearray(_read("rgb256_97_1bpp.j2k"))
+    rng = np.random.default_rng(1)
+    for _ in range(4):
+        bad = bytearray(cs)
+        for pos in rng.integers(len(cs) // 3, len(cs), 30):
+            bad[pos] = int(rng.integers(0, 256))
+        try:
+            plan = native.Plan(bytes(bad))
+        except native.J2kError:
+            continue
+        gpu_ctx.begin()
+        gpu_ctx.add(plan, native.FMT_24BITS_RGB)
+        gpu_ctx.launch()
+        assert gpu_ctx.sync(timeout_ms=20000) == 0
+        orc, oout, _ = oracle_util.oracle_decode(plan, native.FMT_24BITS_RGB)
+        assert np.array_equal(gpu_ctx.output(0), oout)
