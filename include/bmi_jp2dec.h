@@ -10,7 +10,8 @@
  * Semantics here: BMI_dec_info parses the main header into the parameter block and
  * reports pool sizes; BMI_dec_init checks the caller's pools; BMI_dec decodes the whole
  * codestream on the GPU and writes one plane per component into output[c] as
- * DC-shifted, clamped samples (uint8 for bit depths <= 8, uint16 above);
+ * DC-shifted, clamped samples after the inverse MCT (R, G, B for colour pictures;
+ * uint8 for bit depths <= 8, uint16 above);
  * BMI_dec_thumbnail does the same at 1/2^resolution size.
  */
 #ifndef BMI_JP2DEC_H

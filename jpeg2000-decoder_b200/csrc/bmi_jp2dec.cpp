@@ -34,25 +34,46 @@ int decode_planes(stru_dec_param *p, void *output[MAX_COMPONENT], int discard) {
   if (j2k_plan_create((const uint8_t *)p->input, p->in_size, discard, 0, 0, &plan) != J2K_OK) return -1;
   j2k_image_info I;
   j2k_plan_info(plan, &I);
+  // colour pictures come back through the inverse MCT (RGB order), others per component
+  const bool rgb = I.ncomp >= 3 && I.mct;
+  const bool wide = I.bitdepth > 8;
+  const int fmt = rgb ? (wide ? J2K_FMT_48BITS_RGB : J2K_FMT_24BITS_RGB) : J2K_FMT_NONE;
   int rc = -1;
-  if (j2k_gpu_batch_begin(c) == J2K_OK && j2k_gpu_batch_add(c, plan, J2K_FMT_NONE, 0, nullptr) == J2K_OK &&
+  if (j2k_gpu_batch_begin(c) == J2K_OK && j2k_gpu_batch_add(c, plan, fmt, 0, nullptr) == J2K_OK &&
       j2k_gpu_batch_launch(c, nullptr) == J2K_OK && j2k_gpu_batch_sync(c, -1) == J2K_OK) {
     const size_t n = (size_t)I.width * I.height;
-    std::vector<int32_t> tmp(n);
     const int dc = 1 << (I.bitdepth - 1), maxv = (1 << I.bitdepth) - 1;
     rc = j2k_gpu_image_status(c, 0, nullptr) == J2K_OK ? 0 : -1;
-    for (int comp = 0; comp < I.ncomp && comp < MAX_COMPONENT; ++comp) {
-      if (!output[comp]) continue;
-      if (j2k_gpu_component_copy(c, 0, comp, tmp.data(), n * 4) != J2K_OK) {
-        rc = -1;
-        break;
+    if (rgb) {
+      std::vector<uint8_t> px(j2k_output_bytes(&I, fmt));
+      if (j2k_gpu_output_copy(c, 0, px.data(), px.size()) != J2K_OK) rc = -1;
+      // RGB_24BITS / RGB_48BITS store B, G, R; the container holds the LIFTed value
+      for (int comp = 0; comp < 3 && rc == 0; ++comp) {
+        if (!output[comp]) continue;
+        for (size_t i = 0; i < n; ++i) {
+          if (wide) {
+            const uint16_t v = reinterpret_cast<const uint16_t *>(px.data())[i * 3 + (2 - comp)];
+            ((uint16_t *)output[comp])[i] = (uint16_t)(v >> (16 - I.bitdepth));
+          } else {
+            ((uint8_t *)output[comp])[i] = px[i * 3 + (2 - comp)];
+          }
+        }
       }
-      for (size_t i = 0; i < n; ++i) {
-        int v = I.reversible ? tmp[i] : (int)reinterpret_cast<const float *>(tmp.data())[i];
-        v += dc;
-        v = v < 0 ? 0 : (v > maxv ? maxv : v);
-        if (I.bitdepth <= 8) ((uint8_t *)output[comp])[i] = (uint8_t)v;
-        else ((uint16_t *)output[comp])[i] = (uint16_t)v;
+    } else {
+      std::vector<int32_t> tmp(n);
+      for (int comp = 0; comp < I.ncomp && comp < MAX_COMPONENT && rc == 0; ++comp) {
+        if (!output[comp]) continue;
+        if (j2k_gpu_component_copy(c, 0, comp, tmp.data(), n * 4) != J2K_OK) {
+          rc = -1;
+          break;
+        }
+        for (size_t i = 0; i < n; ++i) {
+          int v = I.reversible ? tmp[i] : (int)reinterpret_cast<const float *>(tmp.data())[i];
+          v += dc;
+          v = v < 0 ? 0 : (v > maxv ? maxv : v);
+          if (!wide) ((uint8_t *)output[comp])[i] = (uint8_t)v;
+          else ((uint16_t *)output[comp])[i] = (uint16_t)v;
+        }
       }
     }
   }

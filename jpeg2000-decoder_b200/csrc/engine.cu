@@ -46,31 +46,37 @@ __device__ __forceinline__ int32_t place53(int32_t v, int numbps) {
   return v < 0 ? -(int32_t)((uint32_t)(v & 0x7FFFFFFF) >> sh) : (int32_t)((uint32_t)v >> sh);
 }
 
-template <int MAXW, int MAXH>
+template <int MAXW, int MAXH, typename S>
 struct T1Layout {
   static constexpr int STRIPES = MAXH / 4;
   static constexpr int GAP = MAXW + 3;
   static constexpr int CWN = (STRIPES + 2) * GAP + 2;
-  static constexpr int PER_WARP = ((CWN * 4 + MAXH * MAXW * 4 + 32) + 15) & ~15;
+  static constexpr int SAMPLE_BYTES = MAXH * MAXW * (int)sizeof(S);
+  static constexpr int PER_WARP = ((CWN * 4 + SAMPLE_BYTES + N_CTX * 4) + 15) & ~15;
 };
 
-template <int MAXW, int MAXH>
-__global__ void t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n,
-                          int *__restrict__ counter, const uint8_t *__restrict__ bytes,
-                          const uint32_t *__restrict__ seglens, void *__restrict__ coef, uint16_t *__restrict__ status,
-                          const T1Tables *__restrict__ gtab) {
+// Host-side queue classes: block size bound and sample width
+enum { Q64_16 = 0, Q64_32 = 1, Q32_16 = 2, Q32_32 = 3, NQ = 4 };
+// 16-bit samples hold bit-planes [shift, shift + 14]: at most 14 coded planes (40 passes)
+constexpr int MAX_PASSES_16 = 40;
+
+template <int MAXW, int MAXH, typename S>
+__global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order,
+                                                  int n, int *__restrict__ counter, const uint8_t *__restrict__ bytes,
+                                                  const uint32_t *__restrict__ seglens, void *__restrict__ coef,
+                                                  uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab) {
   extern __shared__ __align__(16) uint8_t smem[];
-  typedef T1Layout<MAXW, MAXH> Lay;
+  typedef T1Layout<MAXW, MAXH, S> Lay;
   T1Tables &T = *reinterpret_cast<T1Tables *>(smem);
   for (int i = threadIdx.x; i < (int)(sizeof(T1Tables) / 4); i += blockDim.x)
     reinterpret_cast<uint32_t *>(smem)[i] = reinterpret_cast<const uint32_t *>(gtab)[i];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t *mine = smem + ((sizeof(T1Tables) + 15) & ~15) + warp * Lay::PER_WARP;
-  BlockSmem b;
+  BlockSmem<S> b;
   b.cw = reinterpret_cast<uint32_t *>(mine);
-  b.sp = reinterpret_cast<int32_t *>(mine + Lay::CWN * 4);
-  b.st = mine + Lay::CWN * 4 + MAXH * MAXW * 4;
+  b.sp.p = reinterpret_cast<S *>(mine + Lay::CWN * 4);
+  b.cx = reinterpret_cast<uint32_t *>(mine + Lay::CWN * 4 + Lay::SAMPLE_BYTES);
   for (;;) {
     int idx = 0;
     if (lane == 0) idx = atomicAdd(counter, 1);
@@ -80,11 +86,19 @@ __global__ void t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__re
     const j2k_cblk cb = cbs[ci];
     b.w = cb.w;
     b.gap = cb.w + 3;
+    int bit_plane, num_passes;
+    block_planes(cb, bit_plane, num_passes);
+    if constexpr (sizeof(S) == 2) {
+      // lowest decoded plane's midpoint bit is the bottom of the 16-bit window; pass 0 is
+      // the top plane's cleanup, every further plane has up to three passes
+      const int planes = (num_passes + 4) / 3;
+      b.sp.shift = max(0, bit_plane - planes);
+    }
     int st;
-    if (cb.w == 0 || cb.h == 0 || cb.w > MAXW || cb.h > MAXH) {
+    if (cb.w == 0 || cb.h == 0 || cb.w > MAXW || cb.h > MAXH || (sizeof(S) == 2 && num_passes > MAX_PASSES_16)) {
       st = 9;
     } else {
-      st = decode_block<MAXW, MAXH>(cb, bytes, seglens, b, T, lane);
+      st = decode_block<S>(cb, bytes, seglens, b, T, lane, bit_plane, num_passes);
     }
     // dequantising (9/7) or shifting (5/3) store into the subband buffer, coalesced by row
     const int w = cb.w, h = cb.h;
@@ -93,13 +107,13 @@ __global__ void t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__re
         float *dst = reinterpret_cast<float *>(coef) + cb.out_off;
         for (int i = lane; i < w * h; i += 32) {
           const int y = i / w, x = i - y * w;
-          dst[(size_t)y * cb.out_stride + x] = __fmul_rn((float)signmag_to_int(b.sp[y * w + x]), cb.gain);
+          dst[(size_t)y * cb.out_stride + x] = __fmul_rn((float)signmag_to_int(b.sp.raw(y * w + x)), cb.gain);
         }
       } else {
         int32_t *dst = reinterpret_cast<int32_t *>(coef) + cb.out_off;
         for (int i = lane; i < w * h; i += 32) {
           const int y = i / w, x = i - y * w;
-          dst[(size_t)y * cb.out_stride + x] = place53(b.sp[y * w + x], cb.mb);
+          dst[(size_t)y * cb.out_stride + x] = place53(b.sp.raw(y * w + x), cb.mb);
         }
       }
     }
@@ -127,7 +141,7 @@ void build_t1_tables(T1Tables &T) {
     int sw = (QE[idx] == 0x5601 && NLPS[idx] != 46);
     uint32_t nm = (uint32_t)(NMPS[idx] << 1 | mps);
     uint32_t nl = (uint32_t)(NLPS[idx] << 1 | (mps ^ sw));
-    T.mq[s] = ((uint32_t)QE[idx] << 16) | (nm << 8) | nl;
+    T.mq[s] = ((uint32_t)QE[idx] << 17) | ((uint32_t)mps << 16) | (nm << 8) | nl;
   }
   for (int band = 0; band < 3; ++band)
     for (int nb = 0; nb < 512; ++nb) {
@@ -201,7 +215,7 @@ struct j2k_gpu_ctx {
   bool launched = false, synced = false, staged = false;
   // staged batch (device-resident inputs) for batch_run
   struct Staged {
-    size_t n_big = 0, n_small = 0, n_cblks = 0, n_otasks = 0;
+    size_t nq[4] = {0, 0, 0, 0}, n_cblks = 0, n_otasks = 0;
     size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0;
     int maxL = 0;
     std::vector<uint32_t> dtask_off;
@@ -292,8 +306,10 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
     return J2K_ERR_CUDA;
   }
   // opt into the large dynamic shared memory of the Tier-1 kernels
-  cudaFuncSetAttribute(t1_kernel<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64, int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<32, 32, int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<32, 32, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   *out = c;
   return J2K_OK;
 }
@@ -394,6 +410,37 @@ extern "C" int j2k_gpu_batch_footprint(const j2k_gpu_ctx *cc, size_t *bytes) {
   return J2K_OK;
 }
 
+namespace {
+// Persistent Tier-1 launch: the CTA shape with the most resident warps per SM (registers,
+// shared memory and thread limits from the occupancy calculator), one wave of CTAs.
+template <int MAXW, int MAXH, typename S>
+void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
+               const uint32_t *seg, const T1Tables *tab) {
+  typedef T1Layout<MAXW, MAXH, S> Lay;
+  const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
+  int best_w = 1, best_ctas = 1, best_warps = 0;
+  const int wmax = c->tuning.t1_warps_per_cta > 0 ? std::min(8, c->tuning.t1_warps_per_cta) : 8;
+  for (int w = 1; w <= wmax; ++w) {
+    const size_t sm = tsz + (size_t)w * Lay::PER_WARP;
+    if (sm > c->smem_optin) break;
+    int ctas = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH, S>, w * 32, sm) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (ctas * w > best_warps || (ctas * w == best_warps && w > best_w)) {
+      best_warps = ctas * w;
+      best_w = w;
+      best_ctas = ctas;
+    }
+  }
+  const size_t sm = tsz + (size_t)best_w * Lay::PER_WARP;
+  const int grid = std::max(1, std::min((n + best_w - 1) / best_w, c->sm_count * std::max(1, best_ctas)));
+  t1_kernel<MAXW, MAXH, S><<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
+                                                           c->d_A.p, (uint16_t *)c->d_status.p, tab);
+}
+}  // namespace
+
 extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   if (!c) return J2K_ERR_ARG;
   if (c->launched && !c->synced) return J2K_ERR_STATE;
@@ -408,7 +455,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   cbs.reserve(S.cblks);
   std::vector<uint32_t> seg;
   seg.reserve(S.segs);
-  std::vector<uint32_t> ord_big, ord_small;
+  std::vector<uint32_t> ordq[NQ];
   std::vector<DwtLevel> levels;
   std::vector<std::vector<DwtTask>> steps_rev, steps_irr;
   std::vector<OutGroup> groups;
@@ -430,8 +477,9 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       uint32_t idx = (uint32_t)cbs.size();
       cbs.push_back(cb);
       if (cb.num_passes == 0 && !(cb.flags & J2K_CB_IRREV) && false) continue;
-      if (cb.w <= 32 && cb.h <= 32) ord_small.push_back(idx);
-      else ord_big.push_back(idx);
+      const bool small = cb.w <= 32 && cb.h <= 32;
+      const bool narrow = cb.num_passes <= MAX_PASSES_16;
+      ordq[small ? (narrow ? Q32_16 : Q32_32) : (narrow ? Q64_16 : Q64_32)].push_back(idx);
     }
     seg.insert(seg.end(), p.seglens.begin(), p.seglens.end());
     byte_base += p.bytes.size();
@@ -505,8 +553,11 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   }
   // work queue order: longest coded length first
   auto by_len = [&](uint32_t a, uint32_t b) { return cbs[a].data_len > cbs[b].data_len; };
-  std::sort(ord_big.begin(), ord_big.end(), by_len);
-  std::sort(ord_small.begin(), ord_small.end(), by_len);
+  size_t n_ord = 0;
+  for (auto &q : ordq) {
+    std::sort(q.begin(), q.end(), by_len);
+    n_ord += q.size();
+  }
   std::vector<uint32_t> dtask_off(2 * maxL + 1, 0);
   std::vector<DwtTask> dtasks;
   for (int s = 0; s < maxL; ++s) {
@@ -520,7 +571,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   // ---- staging layout (pinned)
   size_t o_cbs = 0;
   size_t o_ord = align_up(o_cbs + cbs.size() * sizeof(j2k_cblk), 256);
-  size_t o_seg = align_up(o_ord + (ord_big.size() + ord_small.size()) * 4, 256);
+  size_t o_seg = align_up(o_ord + n_ord * 4, 256);
   size_t o_lev = align_up(o_seg + seg.size() * 4, 256);
   size_t o_dtk = align_up(o_lev + levels.size() * sizeof(DwtLevel), 256);
   size_t o_grp = align_up(o_dtk + dtasks.size() * sizeof(DwtTask), 256);
@@ -540,8 +591,13 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   }
   uint8_t *H = (uint8_t *)c->h_stage;
   std::memcpy(H + o_cbs, cbs.data(), cbs.size() * sizeof(j2k_cblk));
-  std::memcpy(H + o_ord, ord_big.data(), ord_big.size() * 4);
-  std::memcpy(H + o_ord + ord_big.size() * 4, ord_small.data(), ord_small.size() * 4);
+  {
+    size_t off = o_ord;
+    for (auto &q : ordq) {
+      std::memcpy(H + off, q.data(), q.size() * 4);
+      off += q.size() * 4;
+    }
+  }
   std::memcpy(H + o_seg, seg.data(), seg.size() * 4);
   std::memcpy(H + o_lev, levels.data(), levels.size() * sizeof(DwtLevel));
   std::memcpy(H + o_dtk, dtasks.data(), dtasks.size() * sizeof(DwtTask));
@@ -573,8 +629,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   CK(cudaMemcpyAsync(D, H, o_byt, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(c->d_bytes.p, H + o_byt, S.bytes, cudaMemcpyHostToDevice, st));
   CK(cudaEventRecord(c->ev[1], st));
-  c->sg.n_big = ord_big.size();
-  c->sg.n_small = ord_small.size();
+  for (int q = 0; q < NQ; ++q) c->sg.nq[q] = ordq[q].size();
   c->sg.n_cblks = S.cblks;
   c->sg.n_otasks = otasks.size();
   c->sg.o_cbs = o_cbs;
@@ -608,7 +663,7 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
     size_t n;
     size_t size() const { return n; }
     bool empty() const { return n == 0; }
-  } ord_big{G.n_big}, ord_small{G.n_small}, otasks{G.n_otasks};
+  } otasks{G.n_otasks};
   c->launches = 0;
   if (!c->launched) {
     // first run after staging: the staging events already bracket the copies
@@ -624,29 +679,19 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   const uint32_t *d_seg = (const uint32_t *)(D + o_seg);
   int *cnt = (int *)c->d_counter.p;
   const T1Tables *tab = (const T1Tables *)c->d_tables.p;
-  const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
-  if (!ord_big.empty()) {
-    int warps = std::max(1, std::min(c->tuning.t1_warps_per_cta, (int)((c->smem_optin - tsz) / T1Layout<64, 64>::PER_WARP)));
-    size_t sm = tsz + (size_t)warps * T1Layout<64, 64>::PER_WARP;
-    int ctas_per_sm = std::max(1, (int)((228 * 1024) / (sm + 1024)));
-    int grid = std::min((int)((ord_big.size() + warps - 1) / warps), c->sm_count * ctas_per_sm);
-    t1_kernel<64, 64><<<grid, warps * 32, sm, st>>>(d_cbs, d_ord, (int)ord_big.size(), cnt, (const uint8_t *)c->d_bytes.p,
-                                                     d_seg, c->d_A.p, (uint16_t *)c->d_status.p, tab);
-    c->launches++;
-  }
-  if (!ord_small.empty()) {
-    int warps = std::max(1, std::min(2 * c->tuning.t1_warps_per_cta, 32));
-    size_t sm = tsz + (size_t)warps * T1Layout<32, 32>::PER_WARP;
-    while (sm > c->smem_optin && warps > 1) {
-      warps /= 2;
-      sm = tsz + (size_t)warps * T1Layout<32, 32>::PER_WARP;
+  size_t qoff = 0;
+  for (int q = 0; q < NQ; ++q) {
+    const int n = (int)G.nq[q];
+    if (n) {
+      switch (q) {
+        case Q64_16: launch_t1<64, 64, int16_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
+        case Q64_32: launch_t1<64, 64, int32_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
+        case Q32_16: launch_t1<32, 32, int16_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
+        default: launch_t1<32, 32, int32_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
+      }
+      c->launches++;
     }
-    int ctas_per_sm = std::max(1, (int)((228 * 1024) / (sm + 1024)));
-    int grid = std::min((int)((ord_small.size() + warps - 1) / warps), c->sm_count * ctas_per_sm);
-    t1_kernel<32, 32><<<grid, warps * 32, sm, st>>>(d_cbs, d_ord + ord_big.size(), (int)ord_small.size(), cnt + 1,
-                                                     (const uint8_t *)c->d_bytes.p, d_seg, c->d_A.p,
-                                                     (uint16_t *)c->d_status.p, tab);
-    c->launches++;
+    qoff += G.nq[q];
   }
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[2], st));

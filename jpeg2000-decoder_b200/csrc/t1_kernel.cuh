@@ -1,15 +1,25 @@
 /*
  * t1_kernel.cuh — EBCOT Tier-1 code-block decoder for sm_100a.
  *
- * One warp per code-block.  The warp keeps the block's stripe context words and its int32
+ * One warp per code-block.  The warp keeps the block's stripe context words and its
  * samples in shared memory and the MQ registers (A, C, t, T, byte position) in registers.
  * The arithmetic decode is inherently serial, so all 32 lanes execute the same scalar
  * decode in lock-step (uniform control flow, broadcast shared-memory reads); the lanes
  * work in parallel where the data allows it: clearing the state, locating the next
- * non-empty stripe column of a pass with a warp ballot, and the dequantising, coalesced
- * store of the finished block into the subband buffer.  Blocks are pulled from a device
- * work queue (atomic counter over a host-sorted order, longest blocks first), so CTAs
- * stay resident and uneven blocks balance out.
+ * non-empty stripe column of a pass with a warp ballot, measuring runs of empty columns
+ * in the cleanup pass, and the dequantising, coalesced store of the finished block.
+ * Blocks are pulled from a device work queue (atomic counter over a host-sorted order,
+ * longest blocks first), so CTAs stay resident and uneven blocks balance out.
+ *
+ * Latency and occupancy measures, none of which changes a decoded bit:
+ *   - each MQ context slot holds its probability-table entry (Qe, MPS, both successor
+ *     states), so a symbol needs one shared-memory load before its decision;
+ *   - in the cleanup pass a run of all-zero columns whose run-length symbols would all
+ *     decode as MPS without renormalisation (C >= k*Qe and A - k*Qe >= 0x8000, scaled) is
+ *     consumed in one step: A -= k*Qe, C -= k*Qe;
+ *   - blocks with at most 14 coded bit-planes keep their samples in 16 bits (sign + the
+ *     15 magnitude bits from the lowest decoded plane's midpoint bit upward), halving the
+ *     shared memory per warp; deeper blocks use 32-bit samples.
  *
  * Semantics follow the reference block decoder exactly (decoder/codec/src/
  * bmi_block_decoder.cpp:10-853, bmi_mq_decoder.h/.cpp, bmi_t1_macro.h): same context-word
@@ -41,9 +51,10 @@ constexpr uint32_t CHI_ALL = (1u << 19) | (1u << 22) | (1u << 25) | (1u << 28);
 enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, N_CTX = 18 };
 
 // Shared tables, filled once per CTA:
-//   mq[94]  : (Qe << 16) | (next state after MPS << 8) | next state after LPS, state = idx*2+mps
+//   mq[94]   : entry of state s = idx*2 + mps:
+//              (Qe << 17) | (mps << 16) | (state after an MPS << 8) | state after an LPS
 //   zc[3][512]: zero-coding context for LL/LH, HL, HH neighbourhoods
-//   sc[256] : (sign context << 1) | xor bit for an 8-bit (sigma, chi) neighbour index
+//   sc[256]  : (sign context << 1) | xor bit for an 8-bit (sigma, chi) neighbour index
 struct T1Tables {
   uint32_t mq[96];
   uint8_t zc[3][512];
@@ -109,19 +120,18 @@ __device__ __forceinline__ void mq_renorm(Mq &m) {
   }
 }
 
-// MQ_DECODE, bmi_mq_decoder.h:86-128
-__device__ __forceinline__ int mq_decode(Mq &m, uint8_t *st, const uint32_t *tab) {
-  uint32_t s = *st;
-  uint32_t e = tab[s];
-  int32_t q = (int32_t)(e >> 16) << 8;
-  int sym = (int)(s & 1);
+// MQ_DECODE, bmi_mq_decoder.h:86-128, on a context slot holding its table entry
+__device__ __forceinline__ int mq_decode(Mq &m, uint32_t *cx, const uint32_t *tab) {
+  const uint32_t e = *cx;
+  const int32_t q = (int32_t)(e >> 17) << 8;
+  int sym = (int)((e >> 16) & 1);
   m.A -= q;
   if (m.C < q) {
     if (m.A < q) {
-      *st = (uint8_t)(e >> 8);
+      *cx = tab[(e >> 8) & 0xFF];
     } else {
       sym ^= 1;
-      *st = (uint8_t)e;
+      *cx = tab[e & 0xFF];
     }
     m.A = q;
     mq_renorm(m);
@@ -130,9 +140,9 @@ __device__ __forceinline__ int mq_decode(Mq &m, uint8_t *st, const uint32_t *tab
     if (m.A < 0x800000) {
       if (m.A < q) {
         sym ^= 1;
-        *st = (uint8_t)e;
+        *cx = tab[e & 0xFF];
       } else {
-        *st = (uint8_t)(e >> 8);
+        *cx = tab[(e >> 8) & 0xFF];
       }
       mq_renorm(m);
     }
@@ -187,15 +197,66 @@ __device__ __forceinline__ int raw_bit(Raw &r) {
   return (int)((r.c >> r.ct) & 1);
 }
 
+// ---- sample storage: the reference's int32 (bit 31 sign, magnitude) or a 16-bit window
+// (bit 15 sign, magnitude bits [shift, shift + 14])
+template <typename S>
+struct Samples;
+
+template <>
+struct Samples<int32_t> {
+  int32_t *p;
+  __device__ __forceinline__ void set_sig(int i, int sign, int plane) const {
+    const uint32_t oh = (1u << plane) + ((1u << plane) >> 1);
+    p[i] = (int32_t)(((uint32_t)sign << 31) + oh);
+  }
+  __device__ __forceinline__ uint32_t mag_above(int i, int plane) const {
+    return (uint32_t)(p[i] & 0x7FFFFFFF) >> plane;
+  }
+  __device__ __forceinline__ void refine(int i, int sym, int plane) const {
+    int32_t v = p[i];
+    v ^= (int32_t)((uint32_t)(1 - sym) << plane);
+    v |= (int32_t)((1u << plane) >> 1);
+    p[i] = v;
+  }
+  __device__ __forceinline__ int32_t raw(int i) const { return p[i]; }
+  __device__ __forceinline__ void clear(int i) const { p[i] = 0; }
+};
+
+template <>
+struct Samples<int16_t> {
+  int16_t *p;
+  int shift;
+  __device__ __forceinline__ void set_sig(int i, int sign, int plane) const {
+    const uint32_t oh = ((1u << plane) + ((1u << plane) >> 1)) >> shift;
+    p[i] = (int16_t)(((uint32_t)sign << 15) | oh);
+  }
+  __device__ __forceinline__ uint32_t mag_above(int i, int plane) const {
+    return ((uint32_t)(uint16_t)p[i] & 0x7FFF) >> (plane - shift);
+  }
+  __device__ __forceinline__ void refine(int i, int sym, int plane) const {
+    uint32_t v = (uint16_t)p[i];
+    v ^= (uint32_t)(1 - sym) << (plane - shift);
+    v |= ((1u << plane) >> 1) >> shift;
+    p[i] = (int16_t)v;
+  }
+  __device__ __forceinline__ int32_t raw(int i) const {
+    const uint32_t v = (uint16_t)p[i];
+    return (int32_t)(((v & 0x8000u) << 16) | ((v & 0x7FFFu) << shift));
+  }
+  __device__ __forceinline__ void clear(int i) const { p[i] = 0; }
+};
+
 // per-warp decode state in shared memory
+template <typename S>
 struct BlockSmem {
   uint32_t *cw;  // context words: (stripes + 2) rows of (w + 3) words, + 2
-  int32_t *sp;   // samples: (stripes * 4) x w
-  uint8_t *st;   // 18 MQ context states
+  Samples<S> sp; // (stripes * 4) x w samples
+  uint32_t *cx;  // 18 MQ context slots (table entries)
   int w, gap;
 };
 
-__device__ __forceinline__ uint32_t *cword(const BlockSmem &b, int s, int c) {
+template <typename S>
+__device__ __forceinline__ uint32_t *cword(const BlockSmem<S> &b, int s, int c) {
   return b.cw + (s + 1) * b.gap + 1 + c;
 }
 
@@ -212,8 +273,8 @@ __device__ __forceinline__ int sign_index(uint32_t cw, uint32_t wl, uint32_t wr,
 
 // Decode (or read raw) the sign of row k, mark the sample significant and spread sigma /
 // chi to the neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).
-template <bool RAW>
-__device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, Mq &mq, Raw &raw,
+template <bool RAW, typename S>
+__device__ __forceinline__ int decode_sign(const BlockSmem<S> &b, uint32_t *wp, uint32_t &cw, int k, Mq &mq, Raw &raw,
                                            const T1Tables &T) {
   int sym;
   if (RAW) {
@@ -221,7 +282,7 @@ __device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uin
   } else {
     int si = sign_index(cw, wp[-1], wp[1], k);
     int v = T.sc[si];
-    sym = mq_decode(mq, b.st + C_SIGN + (v >> 1), T.mq) ^ (v & 1);
+    sym = mq_decode(mq, b.cx + C_SIGN + (v >> 1), T.mq) ^ (v & 1);
   }
   if (k == 0) {
     uint32_t *up = wp - b.gap;
@@ -241,10 +302,9 @@ __device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uin
 }
 
 // significance propagation (bmi_block_decoder.cpp:10-215)
-template <bool RAW>
-__device__ void pass_sigprop(const BlockSmem &b, int stripes, int p, int band, Mq &mq, Raw &raw, const T1Tables &T,
+template <bool RAW, typename S>
+__device__ void pass_sigprop(const BlockSmem<S> &b, int stripes, int p, int band, Mq &mq, Raw &raw, const T1Tables &T,
                              int lane) {
-  const int32_t one_and_half = (1 << p) + ((1 << p) >> 1);
   const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
   for (int s = 0; s < stripes; ++s) {
     uint32_t *row = cword(b, s, 0);
@@ -265,11 +325,11 @@ __device__ void pass_sigprop(const BlockSmem &b, int stripes, int p, int band, M
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           if ((cw & ROW_NBR(k)) && !(cw & (ROW_SIG(k) | ROW_CHI(k)))) {
-            int sym = RAW ? raw_bit(raw) : mq_decode(mq, b.st + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
+            int sym = RAW ? raw_bit(raw) : mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
             cw |= ROW_PI(k);
             if (sym) {
               int sg = decode_sign<RAW>(b, wp, cw, k, mq, raw, T);
-              b.sp[(4 * s + k) * b.w + col] = (int32_t)(((uint32_t)sg << 31) + (uint32_t)one_and_half);
+              b.sp.set_sig((4 * s + k) * b.w + col, sg, p);
               newsig = true;
             }
           }
@@ -282,9 +342,8 @@ __device__ void pass_sigprop(const BlockSmem &b, int stripes, int p, int band, M
 }
 
 // magnitude refinement (bmi_block_decoder.cpp:217-349)
-template <bool RAW>
-__device__ void pass_magref(const BlockSmem &b, int stripes, int p, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
-  const int32_t half = (1 << p) >> 1;
+template <bool RAW, typename S>
+__device__ void pass_magref(const BlockSmem<S> &b, int stripes, int p, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
   for (int s = 0; s < stripes; ++s) {
     uint32_t *row = cword(b, s, 0);
     for (int c0 = 0; c0 < b.w; c0 += 32) {
@@ -299,56 +358,83 @@ __device__ void pass_magref(const BlockSmem &b, int stripes, int p, Mq &mq, Raw 
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           if ((cw & (ROW_MU(k) | ROW_SIG(k))) == (ROW_MU(k) | ROW_SIG(k))) {
-            int32_t *v = &b.sp[(4 * s + k) * b.w + col];
-            int32_t val = *v;
+            const int i = (4 * s + k) * b.w + col;
             int sym;
             if (RAW) {
               sym = raw_bit(raw);
             } else {
               int ctx = C_MAG;
-              if (((val & 0x7FFFFFFF) >> p) < 4) {
+              if (b.sp.mag_above(i, p) < 4) {
                 if (cw & ROW_NBR(k)) ctx++;
               } else {
                 ctx += 2;
               }
-              sym = mq_decode(mq, b.st + ctx, T.mq);
+              sym = mq_decode(mq, b.cx + ctx, T.mq);
             }
-            val ^= (int32_t)((uint32_t)(1 - sym) << p);
-            val |= half;
-            *v = val;
+            b.sp.refine(i, sym, p);
           }
         }
       }
-      __syncwarp();
     }
   }
 }
 
+// number of consecutive zero context words in row[col, w), counted up to `limit`
+__device__ __forceinline__ int zero_run(const uint32_t *row, int col, int w, int limit, int lane) {
+  int run = 0;
+  while (run < limit && col + run < w) {
+    const int c = col + run + lane;
+    const uint32_t nz = __ballot_sync(0xffffffffu, c >= w || row[c] != 0);
+    if (nz) return min(limit, run + __ffs(nz) - 1);
+    run += 32;
+  }
+  return min(limit, run);
+}
+
 // cleanup with run mode (bmi_block_decoder.cpp:351-586)
-__device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, Mq &mq, const T1Tables &T) {
-  const int32_t one_and_half = (1 << p) + ((1 << p) >> 1);
+template <typename S>
+__device__ void pass_cleanup(const BlockSmem<S> &b, int stripes, int p, int band, Mq &mq, const T1Tables &T,
+                             int lane) {
   const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
   Raw dummy;
   for (int s = 0; s < stripes; ++s) {
     uint32_t *row = cword(b, s, 0);
+    __syncwarp();
     for (int col = 0; col < b.w; ++col) {
       uint32_t *wp = row + col;
       uint32_t cw = *wp;
       int k0 = 0;
       if (cw == 0) {
-        if (!mq_decode(mq, b.st + C_RUN, T.mq)) continue;  // whole column stays insignificant
+        // run of columns whose run-length symbols are MPS (0) without renormalisation
+        const uint32_t e = b.cx[C_RUN];
+        if (!((e >> 16) & 1)) {
+          const int32_t q = (int32_t)(e >> 17) << 8;
+          const int32_t room = mq.A - 0x800000;
+          if (room >= q && mq.C >= q) {
+            const int lim = min(room / q, mq.C / q);
+            __syncwarp();
+            const int k = zero_run(row, col, b.w, lim, lane);
+            if (k > 0) {
+              mq.A -= k * q;
+              mq.C -= k * q;
+              col += k - 1;
+              continue;
+            }
+          }
+        }
+        if (!mq_decode(mq, b.cx + C_RUN, T.mq)) continue;  // whole column stays insignificant
         int r = mq_uniform(mq);
         r = (r << 1) | mq_uniform(mq);
         int sg = decode_sign<false>(b, wp, cw, r, mq, dummy, T);
-        b.sp[(4 * s + r) * b.w + col] = (int32_t)(((uint32_t)sg << 31) + (uint32_t)one_and_half);
+        b.sp.set_sig((4 * s + r) * b.w + col, sg, p);
         k0 = r + 1;
       }
       for (int k = k0; k < 4; ++k) {
         if (cw & (ROW_SIG(k) | ROW_CHI(k) | ROW_PI(k))) continue;
-        int sym = mq_decode(mq, b.st + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
+        int sym = mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
         if (sym) {
           int sg = decode_sign<false>(b, wp, cw, k, mq, dummy, T);
-          b.sp[(4 * s + k) * b.w + col] = (int32_t)(((uint32_t)sg << 31) + (uint32_t)one_and_half);
+          b.sp.set_sig((4 * s + k) * b.w + col, sg, p);
         }
       }
       cw |= (cw << (MU_POS - 4)) & MU_ALL;
@@ -359,11 +445,11 @@ __device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, M
   __syncwarp();
 }
 
-__device__ __forceinline__ void init_states(uint8_t *st) {
+__device__ __forceinline__ void init_states(uint32_t *cx, const uint32_t *tab) {
   // bmi_mq_decoder.cpp:65-79: (state 0, MPS 0) except sig ctx 0 -> state 4, run -> state 3
-  for (int i = 0; i < N_CTX; ++i) st[i] = 0;
-  st[C_SIG] = 4 << 1;
-  st[C_RUN] = 3 << 1;
+  for (int i = 0; i < N_CTX; ++i) cx[i] = tab[0];
+  cx[C_SIG] = tab[4 << 1];
+  cx[C_RUN] = tab[3 << 1];
 }
 
 __device__ __forceinline__ bool seg_starts(int flags, int j) {
@@ -373,14 +459,30 @@ __device__ __forceinline__ bool seg_starts(int flags, int j) {
   return (flags & J2K_CB_BYPASS) && j >= 10 && type != 1;
 }
 
+// MSB plane and pass count of a block (bmi_block_decoder.cpp:603-622, :708-711)
+__device__ __forceinline__ void block_planes(const j2k_cblk &cb, int &bit_plane, int &num_passes) {
+  const int missing = cb.missing;
+  const int p_max = 30 - missing;
+  num_passes = 3 * p_max - 2;
+  if (num_passes > cb.num_passes) num_passes = cb.num_passes;
+  if (cb.flags & J2K_CB_IRREV) {
+    bit_plane = (int)cb.mb - 1 - missing;
+  } else {
+    if (((int)cb.mb - missing) * 3 - 2 <= 0) num_passes = 0;
+    bit_plane = -1 - missing;
+  }
+  if (bit_plane < 0) bit_plane = p_max;
+  if (bit_plane == 0) bit_plane = 1;
+}
+
 // Decode one code-block with the whole warp.  Returns a status (0 ok).
-template <int MAXW, int MAXH>
+template <typename S>
 __device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens,
-                            const BlockSmem &b, const T1Tables &T, int lane) {
+                            const BlockSmem<S> &b, const T1Tables &T, int lane, int bit_plane, int num_passes) {
   const int w = cb.w, h = cb.h;
   const int stripes = (h + 3) >> 2;
   // clear samples and context words; mark OOB columns and a partial last stripe
-  for (int i = lane; i < stripes * 4 * w; i += 32) b.sp[i] = 0;
+  for (int i = lane; i < stripes * 4 * w; i += 32) b.sp.clear(i);
   const int nwords = (stripes + 2) * b.gap + 2;
   for (int i = lane; i < nwords; i += 32) b.cw[i] = 0;
   __syncwarp();
@@ -396,24 +498,9 @@ __device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ byte
                               : ((h & 3) == 2 ? (ROW_CHI(2) | ROW_CHI(3)) : ROW_CHI(3));
     for (int c = lane; c < w; c += 32) *cword(b, stripes - 1, c) = m;
   }
-  if (lane == 0) init_states(b.st);
+  if (lane == 0) init_states(b.cx, T.mq);
   __syncwarp();
-
-  const bool irrev = (cb.flags & J2K_CB_IRREV) != 0;
-  const int missing = cb.missing;
-  const int p_max = 30 - missing;
-  int num_passes = 3 * p_max - 2;
-  if (num_passes > cb.num_passes) num_passes = cb.num_passes;
-  int bit_plane;
-  if (irrev) {
-    bit_plane = (int)cb.mb - 1 - missing;
-  } else {
-    if (((int)cb.mb - missing) * 3 - 2 <= 0) num_passes = 0;
-    bit_plane = -1 - missing;
-  }
-  if (bit_plane < 0) bit_plane = p_max;
-  if (bit_plane == 0) bit_plane = 1;
-  if (num_passes > 0 && p_max <= 0) return 1;
+  if (num_passes > 0 && 30 - (int)cb.missing <= 0) return 1;
 
   const int multi = (cb.flags & (J2K_CB_BYPASS | J2K_CB_TERMALL)) != 0;
   const uint8_t *data = bytes + cb.data_off;
@@ -464,13 +551,13 @@ __device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ byte
       if (israw) pass_magref<true>(b, stripes, bit_plane, mq, raw, T, lane);
       else pass_magref<false>(b, stripes, bit_plane, mq, raw, T, lane);
     } else {
-      pass_cleanup(b, stripes, bit_plane, cb.band, mq, T);
+      pass_cleanup(b, stripes, bit_plane, cb.band, mq, T, lane);
       if (cb.flags & J2K_CB_SEGSYM)
         for (int i = 0; i < 4; ++i) mq_uniform(mq);
     }
     if (cb.flags & J2K_CB_RESET) {
       __syncwarp();
-      if (lane == 0) init_states(b.st);
+      if (lane == 0) init_states(b.cx, T.mq);
       __syncwarp();
     }
   }
