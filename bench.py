@@ -17,7 +17,6 @@ decodes its own copy of the batch; images are independent, no collective on the 
 """
 import argparse
 import ctypes
-import hashlib
 import importlib.util
 import json
 import os
@@ -49,52 +48,10 @@ load_package()
 from jpeg2000_decoder_b200 import native, synth  # noqa: E402
 
 METRIC = "Mpixel/s decoded (batched+served vs plain GPU path); p50/p99 decode latency"
-CACHE = os.environ.get("J2K_BENCH_CACHE", "/tmp/j2k_bench_cache")
-
-
-def _cached(key, make):
-    os.makedirs(CACHE, exist_ok=True)
-    path = os.path.join(CACHE, hashlib.sha1(key.encode()).hexdigest() + ".npz")
-    if os.path.exists(path):
-        d = np.load(path, allow_pickle=False)
-        return [bytes(d["s%d" % i]) for i in range(int(d["n"]))]
-    streams = make()
-    np.savez(path, n=len(streams), **{"s%d" % i: np.frombuffer(s, np.uint8) for i, s in enumerate(streams)})
-    return streams
 
 
 def workload(name, quick=False):
-    """(config dict, list of codestreams, output format)."""
-    if name == "c3":
-        nd = 4 if quick else 16
-        reps = 1 if quick else 4
-        distinct = _cached("c3-v1-%d" % nd, lambda: synth.c3_streams(3, n=nd, workers=os.cpu_count()))
-        streams = [distinct[i % nd] for i in range(nd * reps)]
-        cfg = {"workload": "C3 batched video-frame decode", "frames": len(streams), "distinct_frames": nd,
-               "size": "1920x1080", "components": 3, "bitdepth": 8, "wavelet": "9/7+ICT", "tiles": "512x512",
-               "levels": 5, "codeblock": "64x64", "layers": 3, "layer_bpp": [0.5, 1.0, 2.0]}
-        return cfg, streams, native.FMT_24BITS_RGB
-    if name == "c2":
-        streams = _cached("c2-v1", lambda: [synth.c2_stream(2)])
-        cfg = {"workload": "C2 single 2048x2048 RGB 9/7+ICT ~1 bpp", "frames": 1, "size": "2048x2048",
-               "components": 3, "bitdepth": 8, "wavelet": "9/7+ICT", "levels": 5, "codeblock": "64x64",
-               "layers": 1}
-        return cfg, streams, native.FMT_24BITS_RGB
-    if name == "c4":
-        n = 2 if quick else 16
-        nd = min(n, 4)
-        distinct = _cached("c4-v1-%d" % nd, lambda: synth.c4_streams(4, n=nd, workers=os.cpu_count()))
-        streams = [distinct[i % nd] for i in range(n)]
-        cfg = {"workload": "C4 batched 12-bit lossless", "frames": n, "distinct_frames": nd, "size": "4096x2160",
-               "components": 3, "bitdepth": 12, "wavelet": "5/3+RCT", "levels": 6, "codeblock": "32x32",
-               "layers": 8, "progression": "RPCL", "mode": "BYPASS+RESET"}
-        return cfg, streams, native.FMT_48BITS_RGB
-    if name == "c1":
-        streams = _cached("c1-v1", lambda: [synth.c1_stream(1)])
-        cfg = {"workload": "C1 512x512 gray 5/3 lossless", "frames": 1, "size": "512x512", "components": 1,
-               "bitdepth": 8, "wavelet": "5/3", "levels": 5, "codeblock": "64x64", "layers": 1}
-        return cfg, streams, native.FMT_32BITS_4COMPONENTS
-    raise SystemExit("unknown workload " + name)
+    return synth.workload(name, quick)
 
 
 def parse_all(streams, pool):
