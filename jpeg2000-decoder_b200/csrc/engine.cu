@@ -46,37 +46,36 @@ __device__ __forceinline__ int32_t place53(int32_t v, int numbps) {
   return v < 0 ? -(int32_t)((uint32_t)(v & 0x7FFFFFFF) >> sh) : (int32_t)((uint32_t)v >> sh);
 }
 
-template <int MAXW, int MAXH, typename S>
+template <int MAXW, int MAXH>
 struct T1Layout {
   static constexpr int STRIPES = MAXH / 4;
   static constexpr int GAP = MAXW + 3;
   static constexpr int CWN = (STRIPES + 2) * GAP + 2;
-  static constexpr int SAMPLE_BYTES = MAXH * MAXW * (int)sizeof(S);
-  static constexpr int PER_WARP = ((CWN * 4 + SAMPLE_BYTES + N_CTX * 4) + 15) & ~15;
+  static constexpr int RF_BYTES = ((STRIPES * GAP) + 3) & ~3;
+  static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 4) + 15) & ~15;
 };
 
-// Host-side queue classes: block size bound and sample width
-enum { Q64_16 = 0, Q64_32 = 1, Q32_16 = 2, Q32_32 = 3, NQ = 4 };
-// 16-bit samples hold bit-planes [shift, shift + 14]: at most 14 coded planes (40 passes)
-constexpr int MAX_PASSES_16 = 40;
+// Host-side queue classes: code-block size bound
+enum { Q64 = 0, Q32 = 1, NQ = 2 };
 
-template <int MAXW, int MAXH, typename S>
+template <int MAXW, int MAXH>
 __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order,
-                                                  int n, int *__restrict__ counter, const uint8_t *__restrict__ bytes,
-                                                  const uint32_t *__restrict__ seglens, void *__restrict__ coef,
-                                                  uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab) {
+                                                 int n, int *__restrict__ counter, const uint8_t *__restrict__ bytes,
+                                                 const uint32_t *__restrict__ seglens, void *__restrict__ coef,
+                                                 uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab) {
   extern __shared__ __align__(16) uint8_t smem[];
-  typedef T1Layout<MAXW, MAXH, S> Lay;
+  typedef T1Layout<MAXW, MAXH> Lay;
   T1Tables &T = *reinterpret_cast<T1Tables *>(smem);
   for (int i = threadIdx.x; i < (int)(sizeof(T1Tables) / 4); i += blockDim.x)
     reinterpret_cast<uint32_t *>(smem)[i] = reinterpret_cast<const uint32_t *>(gtab)[i];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t *mine = smem + ((sizeof(T1Tables) + 15) & ~15) + warp * Lay::PER_WARP;
-  BlockSmem<S> b;
+  BlockSmem b;
   b.cw = reinterpret_cast<uint32_t *>(mine);
-  b.sp.p = reinterpret_cast<S *>(mine + Lay::CWN * 4);
-  b.cx = reinterpret_cast<uint32_t *>(mine + Lay::CWN * 4 + Lay::SAMPLE_BYTES);
+  b.rf = mine + Lay::CWN * 4;
+  b.cx = reinterpret_cast<uint32_t *>(mine + Lay::CWN * 4 + Lay::RF_BYTES);
+  b.sp.lane = lane;
   for (;;) {
     int idx = 0;
     if (lane == 0) idx = atomicAdd(counter, 1);
@@ -86,34 +85,35 @@ __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cb
     const j2k_cblk cb = cbs[ci];
     b.w = cb.w;
     b.gap = cb.w + 3;
+    int32_t *blk = reinterpret_cast<int32_t *>(coef) + cb.out_off;
+    b.sp.base = blk;
+    b.sp.stride = cb.out_stride;
     int bit_plane, num_passes;
     block_planes(cb, bit_plane, num_passes);
-    if constexpr (sizeof(S) == 2) {
-      // lowest decoded plane's midpoint bit is the bottom of the 16-bit window; pass 0 is
-      // the top plane's cleanup, every further plane has up to three passes
-      const int planes = (num_passes + 4) / 3;
-      b.sp.shift = max(0, bit_plane - planes);
-    }
     int st;
-    if (cb.w == 0 || cb.h == 0 || cb.w > MAXW || cb.h > MAXH || (sizeof(S) == 2 && num_passes > MAX_PASSES_16)) {
+    if (cb.w == 0 || cb.h == 0 || cb.w > MAXW || cb.h > MAXH) {
       st = 9;
     } else {
-      st = decode_block<S>(cb, bytes, seglens, b, T, lane, bit_plane, num_passes);
+      st = decode_block(cb, bytes, seglens, b, T, lane, bit_plane, num_passes);
     }
-    // dequantising (9/7) or shifting (5/3) store into the subband buffer, coalesced by row
+    // rewrite the block in place: raw sign-magnitude -> dequantised float (9/7) or shifted
+    // integer (5/3); lane 0's atomic updates are made visible first
     const int w = cb.w, h = cb.h;
     if (st != 9) {
+      __threadfence();
+      __syncwarp();
       if (cb.flags & J2K_CB_IRREV) {
-        float *dst = reinterpret_cast<float *>(coef) + cb.out_off;
         for (int i = lane; i < w * h; i += 32) {
           const int y = i / w, x = i - y * w;
-          dst[(size_t)y * cb.out_stride + x] = __fmul_rn((float)signmag_to_int(b.sp.raw(y * w + x)), cb.gain);
+          int32_t *a = blk + (size_t)y * cb.out_stride + x;
+          const int32_t v = __ldcg(a);
+          *reinterpret_cast<float *>(a) = __fmul_rn((float)signmag_to_int(v), cb.gain);
         }
       } else {
-        int32_t *dst = reinterpret_cast<int32_t *>(coef) + cb.out_off;
         for (int i = lane; i < w * h; i += 32) {
           const int y = i / w, x = i - y * w;
-          dst[(size_t)y * cb.out_stride + x] = place53(b.sp.raw(y * w + x), cb.mb);
+          int32_t *a = blk + (size_t)y * cb.out_stride + x;
+          *a = place53(__ldcg(a), cb.mb);
         }
       }
     }
@@ -215,7 +215,7 @@ struct j2k_gpu_ctx {
   bool launched = false, synced = false, staged = false;
   // staged batch (device-resident inputs) for batch_run
   struct Staged {
-    size_t nq[4] = {0, 0, 0, 0}, n_cblks = 0, n_otasks = 0;
+    size_t nq[2] = {0, 0}, n_cblks = 0, n_otasks = 0;
     size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0;
     int maxL = 0;
     std::vector<uint32_t> dtask_off;
@@ -306,10 +306,8 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
     return J2K_ERR_CUDA;
   }
   // opt into the large dynamic shared memory of the Tier-1 kernels
-  cudaFuncSetAttribute(t1_kernel<64, 64, int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<64, 64, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<32, 32, int16_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<32, 32, int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   *out = c;
   return J2K_OK;
 }
@@ -413,10 +411,10 @@ extern "C" int j2k_gpu_batch_footprint(const j2k_gpu_ctx *cc, size_t *bytes) {
 namespace {
 // Persistent Tier-1 launch: the CTA shape with the most resident warps per SM (registers,
 // shared memory and thread limits from the occupancy calculator), one wave of CTAs.
-template <int MAXW, int MAXH, typename S>
+template <int MAXW, int MAXH>
 void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
                const uint32_t *seg, const T1Tables *tab) {
-  typedef T1Layout<MAXW, MAXH, S> Lay;
+  typedef T1Layout<MAXW, MAXH> Lay;
   const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
   int best_w = 1, best_ctas = 1, best_warps = 0;
   const int wmax = c->tuning.t1_warps_per_cta > 0 ? std::min(8, c->tuning.t1_warps_per_cta) : 8;
@@ -424,7 +422,7 @@ void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, cons
     const size_t sm = tsz + (size_t)w * Lay::PER_WARP;
     if (sm > c->smem_optin) break;
     int ctas = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH, S>, w * 32, sm) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH>, w * 32, sm) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
@@ -436,7 +434,7 @@ void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, cons
   }
   const size_t sm = tsz + (size_t)best_w * Lay::PER_WARP;
   const int grid = std::max(1, std::min((n + best_w - 1) / best_w, c->sm_count * std::max(1, best_ctas)));
-  t1_kernel<MAXW, MAXH, S><<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
+  t1_kernel<MAXW, MAXH><<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
                                                            c->d_A.p, (uint16_t *)c->d_status.p, tab);
 }
 }  // namespace
@@ -477,9 +475,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       uint32_t idx = (uint32_t)cbs.size();
       cbs.push_back(cb);
       if (cb.num_passes == 0 && !(cb.flags & J2K_CB_IRREV) && false) continue;
-      const bool small = cb.w <= 32 && cb.h <= 32;
-      const bool narrow = cb.num_passes <= MAX_PASSES_16;
-      ordq[small ? (narrow ? Q32_16 : Q32_32) : (narrow ? Q64_16 : Q64_32)].push_back(idx);
+      ordq[(cb.w <= 32 && cb.h <= 32) ? Q32 : Q64].push_back(idx);
     }
     seg.insert(seg.end(), p.seglens.begin(), p.seglens.end());
     byte_base += p.bytes.size();
@@ -683,12 +679,8 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   for (int q = 0; q < NQ; ++q) {
     const int n = (int)G.nq[q];
     if (n) {
-      switch (q) {
-        case Q64_16: launch_t1<64, 64, int16_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
-        case Q64_32: launch_t1<64, 64, int32_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
-        case Q32_16: launch_t1<32, 32, int16_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
-        default: launch_t1<32, 32, int32_t>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab); break;
-      }
+      if (q == Q64) launch_t1<64, 64>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab);
+      else launch_t1<32, 32>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab);
       c->launches++;
     }
     qoff += G.nq[q];

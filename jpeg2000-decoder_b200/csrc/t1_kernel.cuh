@@ -1,13 +1,13 @@
 /*
  * t1_kernel.cuh — EBCOT Tier-1 code-block decoder for sm_100a.
  *
- * One warp per code-block.  The warp keeps the block's stripe context words and its
- * samples in shared memory and the MQ registers (A, C, t, T, byte position) in registers.
+ * One warp per code-block.  The warp keeps the block's stripe context words in shared
+ * memory and the MQ registers (A, C, t, T, byte position) in registers.
  * The arithmetic decode is inherently serial, so all 32 lanes execute the same scalar
  * decode in lock-step (uniform control flow, broadcast shared-memory reads); the lanes
  * work in parallel where the data allows it: clearing the state, locating the next
  * non-empty stripe column of a pass with a warp ballot, measuring runs of empty columns
- * in the cleanup pass, and the dequantising, coalesced store of the finished block.
+ * in the cleanup pass, and the dequantising, coalesced rewrite of the finished block.
  * Blocks are pulled from a device work queue (atomic counter over a host-sorted order,
  * longest blocks first), so CTAs stay resident and uneven blocks balance out.
  *
@@ -17,9 +17,13 @@
  *   - in the cleanup pass a run of all-zero columns whose run-length symbols would all
  *     decode as MPS without renormalisation (C >= k*Qe and A - k*Qe >= 0x8000, scaled) is
  *     consumed in one step: A -= k*Qe, C -= k*Qe;
- *   - blocks with at most 14 coded bit-planes keep their samples in 16 bits (sign + the
- *     15 magnitude bits from the lowest decoded plane's midpoint bit upward), halving the
- *     shared memory per warp; deeper blocks use 32-bit samples.
+ *   - samples live in the block's own region of the output buffer, not in shared memory:
+ *     they are only written while decoding (significance sets sign + 1.5 * 2^p, a
+ *     refinement flips bit p and sets the new midpoint bit), so one lane issues a
+ *     fire-and-forget atomic XOR per update, and the "first refinement?" context test of
+ *     the reference ((|v| >> p) < 4, true exactly on a sample's first refinement) reads a
+ *     per-sample "refined" bit kept in shared memory.  A 64x64 block then needs 5.9 KB of
+ *     shared memory instead of 13-21 KB, so more blocks are resident per SM.
  *
  * Semantics follow the reference block decoder exactly (decoder/codec/src/
  * bmi_block_decoder.cpp:10-853, bmi_mq_decoder.h/.cpp, bmi_t1_macro.h): same context-word
@@ -197,66 +201,33 @@ __device__ __forceinline__ int raw_bit(Raw &r) {
   return (int)((r.c >> r.ct) & 1);
 }
 
-// ---- sample storage: the reference's int32 (bit 31 sign, magnitude) or a 16-bit window
-// (bit 15 sign, magnitude bits [shift, shift + 14])
-template <typename S>
-struct Samples;
-
-template <>
-struct Samples<int32_t> {
-  int32_t *p;
-  __device__ __forceinline__ void set_sig(int i, int sign, int plane) const {
-    const uint32_t oh = (1u << plane) + ((1u << plane) >> 1);
-    p[i] = (int32_t)(((uint32_t)sign << 31) + oh);
+// ---- samples: raw int32 (bit 31 sign, magnitude with midpoint bit) accumulated in global
+// memory by XOR updates from lane 0; the block region is zeroed before decoding
+struct Samples {
+  int32_t *base;      // the block's first sample in the output buffer
+  uint32_t stride;    // elements per row
+  int lane;
+  __device__ __forceinline__ void xor_at(int row, int col, uint32_t v) const {
+    if (lane == 0) atomicXor(reinterpret_cast<unsigned int *>(base + (size_t)row * stride + col), v);
   }
-  __device__ __forceinline__ uint32_t mag_above(int i, int plane) const {
-    return (uint32_t)(p[i] & 0x7FFFFFFF) >> plane;
+  __device__ __forceinline__ void set_sig(int row, int col, int sign, int plane) const {
+    xor_at(row, col, ((uint32_t)sign << 31) + (1u << plane) + ((1u << plane) >> 1));
   }
-  __device__ __forceinline__ void refine(int i, int sym, int plane) const {
-    int32_t v = p[i];
-    v ^= (int32_t)((uint32_t)(1 - sym) << plane);
-    v |= (int32_t)((1u << plane) >> 1);
-    p[i] = v;
+  __device__ __forceinline__ void refine(int row, int col, int sym, int plane) const {
+    xor_at(row, col, ((uint32_t)(1 - sym) << plane) | ((1u << plane) >> 1));
   }
-  __device__ __forceinline__ int32_t raw(int i) const { return p[i]; }
-  __device__ __forceinline__ void clear(int i) const { p[i] = 0; }
-};
-
-template <>
-struct Samples<int16_t> {
-  int16_t *p;
-  int shift;
-  __device__ __forceinline__ void set_sig(int i, int sign, int plane) const {
-    const uint32_t oh = ((1u << plane) + ((1u << plane) >> 1)) >> shift;
-    p[i] = (int16_t)(((uint32_t)sign << 15) | oh);
-  }
-  __device__ __forceinline__ uint32_t mag_above(int i, int plane) const {
-    return ((uint32_t)(uint16_t)p[i] & 0x7FFF) >> (plane - shift);
-  }
-  __device__ __forceinline__ void refine(int i, int sym, int plane) const {
-    uint32_t v = (uint16_t)p[i];
-    v ^= (uint32_t)(1 - sym) << (plane - shift);
-    v |= ((1u << plane) >> 1) >> shift;
-    p[i] = (int16_t)v;
-  }
-  __device__ __forceinline__ int32_t raw(int i) const {
-    const uint32_t v = (uint16_t)p[i];
-    return (int32_t)(((v & 0x8000u) << 16) | ((v & 0x7FFFu) << shift));
-  }
-  __device__ __forceinline__ void clear(int i) const { p[i] = 0; }
 };
 
 // per-warp decode state in shared memory
-template <typename S>
 struct BlockSmem {
   uint32_t *cw;  // context words: (stripes + 2) rows of (w + 3) words, + 2
-  Samples<S> sp; // (stripes * 4) x w samples
+  uint8_t *rf;   // per stripe column: bit k set once row k has been refined
   uint32_t *cx;  // 18 MQ context slots (table entries)
+  Samples sp;
   int w, gap;
 };
 
-template <typename S>
-__device__ __forceinline__ uint32_t *cword(const BlockSmem<S> &b, int s, int c) {
+__device__ __forceinline__ uint32_t *cword(const BlockSmem &b, int s, int c) {
   return b.cw + (s + 1) * b.gap + 1 + c;
 }
 
@@ -273,8 +244,8 @@ __device__ __forceinline__ int sign_index(uint32_t cw, uint32_t wl, uint32_t wr,
 
 // Decode (or read raw) the sign of row k, mark the sample significant and spread sigma /
 // chi to the neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).
-template <bool RAW, typename S>
-__device__ __forceinline__ int decode_sign(const BlockSmem<S> &b, uint32_t *wp, uint32_t &cw, int k, Mq &mq, Raw &raw,
+template <bool RAW>
+__device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, Mq &mq, Raw &raw,
                                            const T1Tables &T) {
   int sym;
   if (RAW) {
@@ -302,8 +273,8 @@ __device__ __forceinline__ int decode_sign(const BlockSmem<S> &b, uint32_t *wp, 
 }
 
 // significance propagation (bmi_block_decoder.cpp:10-215)
-template <bool RAW, typename S>
-__device__ void pass_sigprop(const BlockSmem<S> &b, int stripes, int p, int band, Mq &mq, Raw &raw, const T1Tables &T,
+template <bool RAW>
+__device__ void pass_sigprop(const BlockSmem &b, int stripes, int p, int band, Mq &mq, Raw &raw, const T1Tables &T,
                              int lane) {
   const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
   for (int s = 0; s < stripes; ++s) {
@@ -329,7 +300,7 @@ __device__ void pass_sigprop(const BlockSmem<S> &b, int stripes, int p, int band
             cw |= ROW_PI(k);
             if (sym) {
               int sg = decode_sign<RAW>(b, wp, cw, k, mq, raw, T);
-              b.sp.set_sig((4 * s + k) * b.w + col, sg, p);
+              b.sp.set_sig(4 * s + k, col, sg, p);
               newsig = true;
             }
           }
@@ -342,10 +313,11 @@ __device__ void pass_sigprop(const BlockSmem<S> &b, int stripes, int p, int band
 }
 
 // magnitude refinement (bmi_block_decoder.cpp:217-349)
-template <bool RAW, typename S>
-__device__ void pass_magref(const BlockSmem<S> &b, int stripes, int p, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
+template <bool RAW>
+__device__ void pass_magref(const BlockSmem &b, int stripes, int p, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
   for (int s = 0; s < stripes; ++s) {
     uint32_t *row = cword(b, s, 0);
+    uint8_t *rrow = b.rf + s * b.gap;
     for (int c0 = 0; c0 < b.w; c0 += 32) {
       __syncwarp();
       int c = c0 + lane;
@@ -355,25 +327,28 @@ __device__ void pass_magref(const BlockSmem<S> &b, int stripes, int p, Mq &mq, R
         live &= live - 1;
         int col = c0 + bit;
         uint32_t cw = row[col];
+        uint32_t refined = rrow[col], now = 0;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           if ((cw & (ROW_MU(k) | ROW_SIG(k))) == (ROW_MU(k) | ROW_SIG(k))) {
-            const int i = (4 * s + k) * b.w + col;
             int sym;
             if (RAW) {
               sym = raw_bit(raw);
             } else {
+              // first refinement of this sample <=> (|v| >> p) < 4 in the reference
               int ctx = C_MAG;
-              if (b.sp.mag_above(i, p) < 4) {
+              if (!((refined >> k) & 1)) {
                 if (cw & ROW_NBR(k)) ctx++;
               } else {
                 ctx += 2;
               }
               sym = mq_decode(mq, b.cx + ctx, T.mq);
             }
-            b.sp.refine(i, sym, p);
+            b.sp.refine(4 * s + k, col, sym, p);
+            now |= 1u << k;
           }
         }
+        rrow[col] = (uint8_t)(refined | now);
       }
     }
   }
@@ -392,8 +367,7 @@ __device__ __forceinline__ int zero_run(const uint32_t *row, int col, int w, int
 }
 
 // cleanup with run mode (bmi_block_decoder.cpp:351-586)
-template <typename S>
-__device__ void pass_cleanup(const BlockSmem<S> &b, int stripes, int p, int band, Mq &mq, const T1Tables &T,
+__device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, Mq &mq, const T1Tables &T,
                              int lane) {
   const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
   Raw dummy;
@@ -426,7 +400,7 @@ __device__ void pass_cleanup(const BlockSmem<S> &b, int stripes, int p, int band
         int r = mq_uniform(mq);
         r = (r << 1) | mq_uniform(mq);
         int sg = decode_sign<false>(b, wp, cw, r, mq, dummy, T);
-        b.sp.set_sig((4 * s + r) * b.w + col, sg, p);
+        b.sp.set_sig(4 * s + r, col, sg, p);
         k0 = r + 1;
       }
       for (int k = k0; k < 4; ++k) {
@@ -434,7 +408,7 @@ __device__ void pass_cleanup(const BlockSmem<S> &b, int stripes, int p, int band
         int sym = mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
         if (sym) {
           int sg = decode_sign<false>(b, wp, cw, k, mq, dummy, T);
-          b.sp.set_sig((4 * s + k) * b.w + col, sg, p);
+          b.sp.set_sig(4 * s + k, col, sg, p);
         }
       }
       cw |= (cw << (MU_POS - 4)) & MU_ALL;
@@ -476,15 +450,20 @@ __device__ __forceinline__ void block_planes(const j2k_cblk &cb, int &bit_plane,
 }
 
 // Decode one code-block with the whole warp.  Returns a status (0 ok).
-template <typename S>
 __device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens,
-                            const BlockSmem<S> &b, const T1Tables &T, int lane, int bit_plane, int num_passes) {
+                            const BlockSmem &b, const T1Tables &T, int lane, int bit_plane, int num_passes) {
   const int w = cb.w, h = cb.h;
   const int stripes = (h + 3) >> 2;
-  // clear samples and context words; mark OOB columns and a partial last stripe
-  for (int i = lane; i < stripes * 4 * w; i += 32) b.sp.clear(i);
+  // clear the block's samples (output region), context words and refinement bits; mark
+  // OOB columns and a partial last stripe
+  for (int i = lane; i < w * h; i += 32) {
+    const int y = i / w, x = i - y * w;
+    b.sp.base[(size_t)y * b.sp.stride + x] = 0;
+  }
   const int nwords = (stripes + 2) * b.gap + 2;
   for (int i = lane; i < nwords; i += 32) b.cw[i] = 0;
+  for (int i = lane; i < stripes * b.gap; i += 32) b.rf[i] = 0;
+  __threadfence();  // the zeros reach L2 before lane 0's atomic updates
   __syncwarp();
   const uint32_t oob = CHI_ALL;
   for (int s = lane; s < stripes; s += 32) {
