@@ -134,6 +134,22 @@ typedef struct j2k_gpu_tuning {
 int j2k_gpu_set_tuning(j2k_gpu_ctx *ctx, const j2k_gpu_tuning *t);
 int j2k_gpu_get_tuning(const j2k_gpu_ctx *ctx, j2k_gpu_tuning *t);
 
+/* Inverse DWT of one tile-component that allocates no device memory, for callers that
+ * cannot call cudaMalloc (inside stream capture, in real-time callbacks, or under a host
+ * that owns every device buffer).  No counterpart in the reference.  `coef`: device
+ * pointer to the tile-component's Tier-1 coefficients in the plan's Mallat layout (row
+ * stride tc->w; int32 for 5/3, float for 9/7, as j2k_gpu_coefficients_copy stage 0 lays
+ * them out); `out`: device pointer receiving the reconstructed samples (row stride
+ * `out_stride` elements, the values of j2k_gpu_component_copy).  Intermediate levels use a
+ * static device array of J2K_NOALLOC_SCRATCH_BYTES held by every GPU that loads the
+ * library; tile-components needing more than that (2 * res_w[L-1] * res_h[L-1] * 4 bytes)
+ * return J2K_ERR_UNSUPPORTED.  The first call on a device looks up the array's device
+ * address (make it before any stream capture); overlapping calls race on the array.
+ * Asynchronous on `stream`. */
+#define J2K_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int j2k_gpu_tile_idwt_noalloc(const j2k_tilecomp *tc, int reversible, int flags, const void *coef, void *out,
+                              int out_stride, void *stream);
+
 /* One-call convenience: decode one codestream into host memory (pinned staging inside). */
 int j2k_gpu_decode(j2k_gpu_ctx *ctx, const uint8_t *codestream, size_t len, int out_format, int flags,
                    void *host_out, size_t host_out_bytes);

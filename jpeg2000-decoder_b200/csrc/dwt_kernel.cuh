@@ -235,6 +235,7 @@ __device__ __forceinline__ void put_slot(uint8_t *px, int pxb, int slot, int v) 
   else ((uint16_t *)px)[3 - slot] = (uint16_t)v;
 }
 
+#ifndef J2K_DWT_LEVELS_ONLY
 // Inverse RCT / ICT + DC level shift + clamp + LIFT + pack (bmi_cpu_dwt_decoder.cpp
 // RICT_97_FLOAT :3570-3643, RRct_53 :3936-4130, MergeComponents :4283-4598).
 __global__ void __launch_bounds__(256) output_kernel(const OutGroup *__restrict__ groups,
@@ -312,6 +313,83 @@ __global__ void __launch_bounds__(256) output_kernel(const OutGroup *__restrict_
       }
       for (int k = 0; k < pxb; ++k) px[k] = tmp[k];
     }
+  }
+}
+#endif  // J2K_DWT_LEVELS_ONLY
+
+}  // namespace j2k_dev
+
+namespace j2k_dev {
+
+// One level of one tile-component with every buffer given explicitly (no descriptor
+// tables in device memory): the CTA index selects the 64x64 output tile.  Used by the
+// entry point that runs on a static scratch array (noalloc.cu).
+template <bool REV>
+__global__ void __launch_bounds__(256) dwt_level_explicit_kernel(
+    const typename DwtTypes<REV>::T *__restrict__ quad, int stride_q, const typename DwtTypes<REV>::T *llsrc,
+    int stride_ll, typename DwtTypes<REV>::T *out, int stride_out, int rw, int rh, int lw, int lh, int ll_gain,
+    float ll_gain_value, int refcompat) {
+  typedef typename DwtTypes<REV>::T T;
+  __shared__ T tile[DWT_N * DWT_PITCH];
+  __shared__ T keep[2][DWT_T];
+  const int tiles_x = (rw + DWT_T - 1) / DWT_T;
+  const int ox = (blockIdx.x % tiles_x) * DWT_T, oy = (blockIdx.x / tiles_x) * DWT_T;
+  for (int i = threadIdx.x; i < DWT_N * DWT_N; i += blockDim.x) {
+    const int iy = i / DWT_N, ix = i % DWT_N;
+    const int y = mirror(oy - DWT_H + iy, rh);
+    const int x = mirror(ox - DWT_H + ix, rw);
+    const int sy = (y & 1) ? lh + (y >> 1) : (y >> 1);
+    const int sx = (x & 1) ? lw + (x >> 1) : (x >> 1);
+    T v;
+    if (!(x & 1) && !(y & 1)) {
+      v = llsrc[(size_t)sy * stride_ll + sx];
+      if (!REV && ll_gain) v = (T)__fmul_rn((float)v, ll_gain_value);
+    } else {
+      v = quad[(size_t)sy * stride_q + sx];
+    }
+    tile[iy * DWT_PITCH + ix] = v;
+  }
+  __syncthreads();
+  if (rw > 1) lift_tile<REV, true>(tile, 0, DWT_N);
+  const int n = rh;
+  const bool fix = REV && refcompat && n >= 3 && (oy <= n - 1) && (n - 2 < oy + DWT_T);
+  int rowA = -1, rowB = -1;
+  if (fix) {
+    if (!(n & 1)) {
+      rowA = n - 3;
+    } else {
+      const int m = (n + 1) / 2;
+      rowA = n - 3;
+      rowB = (m >= 3) ? n - 4 : 1;
+    }
+    for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
+      keep[0][c] = tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+      if (rowB >= 0) keep[1][c] = tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+    }
+    __syncthreads();
+  }
+  if (rh > 1) lift_tile<REV, false>(tile, DWT_H, DWT_H + DWT_T);
+  if constexpr (REV) {
+    if (fix) {
+      for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
+        T *col = tile + DWT_H + c;
+        const int r1 = n - 1 - oy + DWT_H, r2 = n - 2 - oy + DWT_H, r3 = n - 3 - oy + DWT_H;
+        if (!(n & 1)) {
+          col[r1 * DWT_PITCH] = keep[0][c] + col[r2 * DWT_PITCH];
+        } else {
+          const T hx = keep[1][c];
+          const T x1 = keep[0][c] - ((hx + 1) >> 1);
+          col[r1 * DWT_PITCH] = x1;
+          col[r2 * DWT_PITCH] = hx + ((x1 + col[r3 * DWT_PITCH]) >> 1);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  const int ow = min(DWT_T, rw - ox), oh = min(DWT_T, rh - oy);
+  for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
+    const int yy = i / DWT_T, xx = i % DWT_T;
+    if (yy < oh && xx < ow) out[(size_t)(oy + yy) * stride_out + ox + xx] = tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
   }
 }
 

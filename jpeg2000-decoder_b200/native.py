@@ -88,7 +88,7 @@ EXPORTS = [
     "j2k_gpu_batch_add", "j2k_gpu_batch_footprint", "j2k_gpu_batch_launch", "j2k_gpu_batch_stage", "j2k_gpu_batch_run", "j2k_gpu_batch_sync",
     "j2k_gpu_image_status", "j2k_gpu_output_device", "j2k_gpu_output_copy", "j2k_gpu_component_copy",
     "j2k_gpu_coefficients_copy", "j2k_gpu_last_timing", "j2k_gpu_last_launches", "j2k_gpu_set_tuning",
-    "j2k_gpu_get_tuning", "j2k_gpu_decode",
+    "j2k_gpu_get_tuning", "j2k_gpu_decode", "j2k_gpu_tile_idwt_noalloc",
     "BMI_dec_info", "BMI_dec_init", "BMI_dec_isr", "BMI_dec", "BMI_dec_thumbnail", "BMI_dec_exit",
     "bmi_decoder_init", "bmi_decoder_set_job", "bmi_decoder_decode", "bmi_decoder_predecode",
     "bmi_decoder_status", "bmi_decoder_result", "bmi_decoder_thumbnail", "bmi_decoder_component_int",
@@ -136,6 +136,7 @@ def lib():
         L.j2k_gpu_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.j2k_gpu_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.j2k_gpu_decode.argtypes = [vp, ctypes.c_char_p, sz, i, i, vp, sz]
+        L.j2k_gpu_tile_idwt_noalloc.argtypes = [ctypes.POINTER(TileComp), i, i, vp, vp, i, vp]
         L.bmi_decoder_init.argtypes = [i, i]
         L.bmi_decoder_set_job.argtypes = [i, i, ctypes.c_uint, i]
         L.bmi_decoder_set_job.restype = None
