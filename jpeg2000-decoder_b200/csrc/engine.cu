@@ -52,7 +52,7 @@ struct T1Layout {
   static constexpr int GAP = MAXW + 3;
   static constexpr int CWN = (STRIPES + 2) * GAP + 2;
   static constexpr int RF_BYTES = ((STRIPES * GAP) + 3) & ~3;
-  static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 4) + 15) & ~15;
+  static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 8) + 15) & ~15;
 };
 
 // Host-side queue classes: code-block size bound
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cb
   BlockSmem b;
   b.cw = reinterpret_cast<uint32_t *>(mine);
   b.rf = mine + Lay::CWN * 4;
-  b.cx = reinterpret_cast<uint32_t *>(mine + Lay::CWN * 4 + Lay::RF_BYTES);
+  b.cx = reinterpret_cast<uint2 *>(mine + Lay::CWN * 4 + Lay::RF_BYTES);
   b.sp.lane = lane;
   for (;;) {
     int idx = 0;
@@ -141,7 +141,8 @@ void build_t1_tables(T1Tables &T) {
     int sw = (QE[idx] == 0x5601 && NLPS[idx] != 46);
     uint32_t nm = (uint32_t)(NMPS[idx] << 1 | mps);
     uint32_t nl = (uint32_t)(NLPS[idx] << 1 | (mps ^ sw));
-    T.mq[s] = ((uint32_t)QE[idx] << 17) | ((uint32_t)mps << 16) | (nm << 8) | nl;
+    T.mq[s].x = (uint32_t)QE[idx] << 8;
+    T.mq[s].y = ((uint32_t)mps << 16) | (nm << 8) | nl;
   }
   for (int band = 0; band < 3; ++band)
     for (int nb = 0; nb < 512; ++nb) {

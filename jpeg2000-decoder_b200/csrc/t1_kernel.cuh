@@ -38,6 +38,10 @@
 
 #include "plan.h"
 
+#ifndef J2K_T1_RED_VARIANT
+#define J2K_T1_RED_VARIANT 0
+#endif
+
 namespace j2k_dev {
 
 // ---- context-word bits (bmi_t1_macro.h:14-73)
@@ -55,12 +59,12 @@ constexpr uint32_t CHI_ALL = (1u << 19) | (1u << 22) | (1u << 25) | (1u << 28);
 enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, N_CTX = 18 };
 
 // Shared tables, filled once per CTA:
-//   mq[94]   : entry of state s = idx*2 + mps:
-//              (Qe << 17) | (mps << 16) | (state after an MPS << 8) | state after an LPS
+//   mq[94]   : entry of state s = idx*2 + mps: .x = Qe << 8 (the scaled register unit),
+//              .y = (mps << 16) | (state after an MPS << 8) | state after an LPS
 //   zc[3][512]: zero-coding context for LL/LH, HL, HH neighbourhoods
 //   sc[256]  : (sign context << 1) | xor bit for an 8-bit (sigma, chi) neighbour index
 struct T1Tables {
-  uint32_t mq[96];
+  uint2 mq[96];
   uint8_t zc[3][512];
   uint8_t sc[256];
 };
@@ -125,17 +129,17 @@ __device__ __forceinline__ void mq_renorm(Mq &m) {
 }
 
 // MQ_DECODE, bmi_mq_decoder.h:86-128, on a context slot holding its table entry
-__device__ __forceinline__ int mq_decode(Mq &m, uint32_t *cx, const uint32_t *tab) {
-  const uint32_t e = *cx;
-  const int32_t q = (int32_t)(e >> 17) << 8;
-  int sym = (int)((e >> 16) & 1);
+__device__ __forceinline__ int mq_decode(Mq &m, uint2 *cx, const uint2 *tab) {
+  const uint2 e = *cx;
+  const int32_t q = (int32_t)e.x;
+  int sym = (int)((e.y >> 16) & 1);
   m.A -= q;
   if (m.C < q) {
     if (m.A < q) {
-      *cx = tab[(e >> 8) & 0xFF];
+      *cx = tab[(e.y >> 8) & 0xFF];
     } else {
       sym ^= 1;
-      *cx = tab[e & 0xFF];
+      *cx = tab[e.y & 0xFF];
     }
     m.A = q;
     mq_renorm(m);
@@ -144,9 +148,9 @@ __device__ __forceinline__ int mq_decode(Mq &m, uint32_t *cx, const uint32_t *ta
     if (m.A < 0x800000) {
       if (m.A < q) {
         sym ^= 1;
-        *cx = tab[e & 0xFF];
+        *cx = tab[e.y & 0xFF];
       } else {
-        *cx = tab[(e >> 8) & 0xFF];
+        *cx = tab[(e.y >> 8) & 0xFF];
       }
       mq_renorm(m);
     }
@@ -207,8 +211,19 @@ struct Samples {
   int32_t *base;      // the block's first sample in the output buffer
   uint32_t stride;    // elements per row
   int lane;
+  // one reduction issued by lane 0; the warp does not wait for it
   __device__ __forceinline__ void xor_at(int row, int col, uint32_t v) const {
-    if (lane == 0) atomicXor(reinterpret_cast<unsigned int *>(base + (size_t)row * stride + col), v);
+    unsigned int *a = reinterpret_cast<unsigned int *>(base + (size_t)row * stride + col);
+#if J2K_T1_RED_VARIANT == 0
+    if (lane == 0) atomicXor(a, v);
+#elif J2K_T1_RED_VARIANT == 1
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.eq.s32 p, %2, 0;\n\t@p red.relaxed.gpu.global.xor.b32 [%0], %1;\n\t}" ::"l"(a),
+                 "r"(v), "r"(lane)
+                 : "memory");
+#else
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.eq.s32 p, %2, 0;\n\t@p red.relaxed.gpu.global.xor.b32 [%0], %1;\n\t}" ::"l"(a),
+                 "r"(v), "r"(lane));
+#endif
   }
   __device__ __forceinline__ void set_sig(int row, int col, int sign, int plane) const {
     xor_at(row, col, ((uint32_t)sign << 31) + (1u << plane) + ((1u << plane) >> 1));
@@ -222,7 +237,7 @@ struct Samples {
 struct BlockSmem {
   uint32_t *cw;  // context words: (stripes + 2) rows of (w + 3) words, + 2
   uint8_t *rf;   // per stripe column: bit k set once row k has been refined
-  uint32_t *cx;  // 18 MQ context slots (table entries)
+  uint2 *cx;     // 18 MQ context slots (table entries)
   Samples sp;
   int w, gap;
 };
@@ -380,9 +395,9 @@ __device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, M
       int k0 = 0;
       if (cw == 0) {
         // run of columns whose run-length symbols are MPS (0) without renormalisation
-        const uint32_t e = b.cx[C_RUN];
-        if (!((e >> 16) & 1)) {
-          const int32_t q = (int32_t)(e >> 17) << 8;
+        const uint2 e = b.cx[C_RUN];
+        if (!((e.y >> 16) & 1)) {
+          const int32_t q = (int32_t)e.x;
           const int32_t room = mq.A - 0x800000;
           if (room >= q && mq.C >= q) {
             const int lim = min(room / q, mq.C / q);
@@ -419,7 +434,7 @@ __device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, M
   __syncwarp();
 }
 
-__device__ __forceinline__ void init_states(uint32_t *cx, const uint32_t *tab) {
+__device__ __forceinline__ void init_states(uint2 *cx, const uint2 *tab) {
   // bmi_mq_decoder.cpp:65-79: (state 0, MPS 0) except sig ctx 0 -> state 4, run -> state 3
   for (int i = 0; i < N_CTX; ++i) cx[i] = tab[0];
   cx[C_SIG] = tab[4 << 1];

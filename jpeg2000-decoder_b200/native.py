@@ -11,7 +11,7 @@ import os
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libj2k_b200.so")
+LIB_PATH = os.environ.get("J2K_B200_LIB") or os.path.join(PKG, "libj2k_b200.so")
 ENC_PATH = os.path.join(PKG, "libj2kenc.so")
 
 # OutputFormat (reference codec_datatype.h)
