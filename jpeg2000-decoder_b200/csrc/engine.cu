@@ -102,18 +102,13 @@ __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cb
     if (st != 9) {
       __threadfence();
       __syncwarp();
-      if (cb.flags & J2K_CB_IRREV) {
-        for (int i = lane; i < w * h; i += 32) {
-          const int y = i / w, x = i - y * w;
-          int32_t *a = blk + (size_t)y * cb.out_stride + x;
-          const int32_t v = __ldcg(a);
-          *reinterpret_cast<float *>(a) = __fmul_rn((float)signmag_to_int(v), cb.gain);
-        }
-      } else {
-        for (int i = lane; i < w * h; i += 32) {
-          const int y = i / w, x = i - y * w;
-          int32_t *a = blk + (size_t)y * cb.out_stride + x;
-          *a = place53(__ldcg(a), cb.mb);
+      const bool irrev = (cb.flags & J2K_CB_IRREV) != 0;
+      for (int y = 0; y < h; ++y) {
+        int32_t *r = blk + (size_t)y * cb.out_stride;
+        for (int x = lane; x < w; x += 32) {
+          const int32_t v = __ldcg(r + x);
+          if (irrev) *reinterpret_cast<float *>(r + x) = __fmul_rn((float)signmag_to_int(v), cb.gain);
+          else r[x] = place53(v, cb.mb);
         }
       }
     }

@@ -12,8 +12,14 @@
  * longest blocks first), so CTAs stay resident and uneven blocks balance out.
  *
  * Latency and occupancy measures, none of which changes a decoded bit:
+ *   - the kernel is kept small for the instruction cache (many resident warps sit in
+ *     different passes at once): each pass visits the four rows of a stripe column in a
+ *     loop rather than unrolled, inlines each of its decisions once, and bypass (raw) and
+ *     MQ decisions share the pass code; one renormalisation site per MQ decision;
  *   - each MQ context slot holds its probability-table entry (Qe, MPS, both successor
  *     states), so a symbol needs one shared-memory load before its decision;
+ *   - code bytes are read as aligned 32-bit words with the next word requested early, so
+ *     byte fills do not wait on memory;
  *   - in the cleanup pass a run of all-zero columns whose run-length symbols would all
  *     decode as MPS without renormalisation (C >= k*Qe and A - k*Qe >= 0x8000, scaled) is
  *     consumed in one step: A -= k*Qe, C -= k*Qe;
@@ -42,6 +48,7 @@
 #define J2K_T1_RED_VARIANT 0
 #endif
 
+
 namespace j2k_dev {
 
 // ---- context-word bits (bmi_t1_macro.h:14-73)
@@ -56,7 +63,7 @@ constexpr uint32_t MU_ALL = (1u << 20) | (1u << 23) | (1u << 26) | (1u << 29);
 constexpr uint32_t PI_ALL = (1u << 21) | (1u << 24) | (1u << 27) | (1u << 30);
 constexpr uint32_t CHI_ALL = (1u << 19) | (1u << 22) | (1u << 25) | (1u << 28);
 
-enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, N_CTX = 18 };
+enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, C_UNI = 18, N_CTX = 19 };
 
 // Shared tables, filled once per CTA:
 //   mq[94]   : entry of state s = idx*2 + mps: .x = Qe << 8 (the scaled register unit),
@@ -69,40 +76,51 @@ struct T1Tables {
   uint8_t sc[256];
 };
 
+// MQ decoder registers.  Code bytes are read as aligned 32-bit words: `cur` holds the byte
+// at `ap`, and the word after it is requested as soon as `cur` is entered, so the load has
+// several fills (dozens of symbols) to complete before its first byte is needed.
 struct Mq {
   int32_t A, C;
   int32_t t, T;
-  uint32_t pos, end;
-  const uint8_t *base;
+  uint32_t ap, aend;  // byte position and segment end, counted from `w`
+  const uint32_t *w;  // the segment's first byte rounded down to a 4-byte boundary
+  uint32_t cur, nxt;  // the word holding byte ap and the one after it
 };
 
-__device__ __forceinline__ int mq_byte(const Mq &m) { return m.pos < m.end ? (int)__ldg(m.base + m.pos) : 0xFF; }
+__device__ __forceinline__ int mq_byte(const Mq &m) {
+  return m.ap < m.aend ? (int)((m.cur >> ((m.ap & 3) * 8)) & 0xFF) : 0xFF;
+}
 
-// FILL_LSBS, bmi_mq_decoder.h:52-73
-__device__ __forceinline__ void mq_fill(Mq &m) {
-  if (m.T == 0xFF) {
-    int b = mq_byte(m);
-    if (b > 0x8F) {
-      m.t = 8;
-    } else {
-      m.T = b << 1;
-      m.pos++;
-      m.t = 7;
-    }
-  } else {
-    m.T = mq_byte(m);
-    m.pos++;
-    m.t = 8;
+__device__ __forceinline__ void mq_advance(Mq &m) {
+  m.ap++;
+  if (!(m.ap & 3)) {
+    m.cur = m.nxt;
+    m.nxt = __ldg(m.w + (m.ap >> 2) + 1);
   }
+}
+
+// FILL_LSBS, bmi_mq_decoder.h:52-73, as selects: after a 0xFF byte the next byte carries 7
+// bits, unless it is a marker (> 0x8F), which is not consumed and reads as 0xFF with 8 bits
+__device__ __forceinline__ void mq_fill(Mq &m) {
+  const int b = mq_byte(m);
+  const bool ff = m.T == 0xFF;
+  const bool marker = ff && b > 0x8F;
+  m.T = marker ? 0xFF : (ff ? b << 1 : b);
+  if (!marker) mq_advance(m);
+  m.t = (ff && !marker) ? 7 : 8;
   m.C += m.T;
 }
 
 // Init, bmi_mq_decoder.cpp:186-219 (the 0xFF 0xFF termination is virtual: bytes at or past
-// `end` read as 0xFF)
+// `end` read as 0xFF).  The word loads may reach up to 9 bytes past the segment; the code
+// byte buffer carries 16 bytes of slack after its last segment.
 __device__ __forceinline__ void mq_init(Mq &m, const uint8_t *base, uint32_t len) {
-  m.base = base;
-  m.pos = 0;
-  m.end = len;
+  const uint32_t off = (uint32_t)((uintptr_t)base & 3);
+  m.w = reinterpret_cast<const uint32_t *>(base - off);
+  m.ap = off;
+  m.aend = off + len;
+  m.cur = __ldg(m.w);
+  m.nxt = __ldg(m.w + 1);
   m.T = 0;
   m.C = 0;
   m.t = 0;
@@ -115,45 +133,36 @@ __device__ __forceinline__ void mq_init(Mq &m, const uint8_t *base, uint32_t len
 }
 
 // Shift until A >= 0x800000, filling a byte whenever t reaches 0 (the reference's
-// RENORMALIZE_ONCE loop, taken several shifts at a time)
+// RENORMALIZE_ONCE loop, taken several shifts at a time; at most two fills, as a fill
+// after a 0xFF byte is followed by one of 8 bits)
 __device__ __forceinline__ void mq_renorm(Mq &m) {
   int n = __clz(m.A) - 8;
-  while (n > 0) {
-    if (m.t == 0) mq_fill(m);
-    int k = min(n, m.t);
-    m.A <<= k;
-    m.C <<= k;
-    m.t -= k;
-    n -= k;
+  while (m.t < n) {
+    m.A <<= m.t;
+    m.C <<= m.t;
+    n -= m.t;
+    mq_fill(m);
   }
+  m.A <<= n;
+  m.C <<= n;
+  m.t -= n;
 }
 
-// MQ_DECODE, bmi_mq_decoder.h:86-128, on a context slot holding its table entry
+// MQ_DECODE, bmi_mq_decoder.h:86-128, on a context slot holding its table entry.  Both
+// renormalising outcomes (conditional exchange after C < Qe; A below 0x8000 after C >= Qe)
+// share one table update and one renormalisation.
 __device__ __forceinline__ int mq_decode(Mq &m, uint2 *cx, const uint2 *tab) {
   const uint2 e = *cx;
   const int32_t q = (int32_t)e.x;
-  int sym = (int)((e.y >> 16) & 1);
   m.A -= q;
-  if (m.C < q) {
-    if (m.A < q) {
-      *cx = tab[(e.y >> 8) & 0xFF];
-    } else {
-      sym ^= 1;
-      *cx = tab[e.y & 0xFF];
-    }
-    m.A = q;
+  const bool ex = m.C < q;
+  const bool lps = ex ? (m.A >= q) : (m.A < q);
+  const int sym = (int)((e.y >> 16) & 1) ^ (int)lps;
+  if (!ex) m.C -= q;
+  if (ex || m.A < 0x800000) {
+    *cx = tab[lps ? (e.y & 0xFF) : ((e.y >> 8) & 0xFF)];
+    if (ex) m.A = q;
     mq_renorm(m);
-  } else {
-    m.C -= q;
-    if (m.A < 0x800000) {
-      if (m.A < q) {
-        sym ^= 1;
-        *cx = tab[e.y & 0xFF];
-      } else {
-        *cx = tab[(e.y >> 8) & 0xFF];
-      }
-      mq_renorm(m);
-    }
   }
   return sym;
 }
@@ -257,19 +266,9 @@ __device__ __forceinline__ int sign_index(uint32_t cw, uint32_t wl, uint32_t wr,
   return (int)idx;
 }
 
-// Decode (or read raw) the sign of row k, mark the sample significant and spread sigma /
-// chi to the neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).
-template <bool RAW>
-__device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, Mq &mq, Raw &raw,
-                                           const T1Tables &T) {
-  int sym;
-  if (RAW) {
-    sym = raw_bit(raw);
-  } else {
-    int si = sign_index(cw, wp[-1], wp[1], k);
-    int v = T.sc[si];
-    sym = mq_decode(mq, b.cx + C_SIGN + (v >> 1), T.mq) ^ (v & 1);
-  }
+// Mark row k of the column at `wp` significant with sign `sym`: spread sigma / chi to the
+// neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).
+__device__ __forceinline__ void spread_sig(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, int sym) {
   if (k == 0) {
     uint32_t *up = wp - b.gap;
     up[-1] |= 0x100u << 9;
@@ -284,151 +283,158 @@ __device__ __forceinline__ int decode_sign(const BlockSmem &b, uint32_t *wp, uin
   wp[-1] |= 0x20u << (3 * k);
   wp[1] |= 0x08u << (3 * k);
   cw |= ROW_SIG(k) | ((uint32_t)sym << (CHI_POS + 3 * k));
-  return sym;
 }
 
-// significance propagation (bmi_block_decoder.cpp:10-215)
-template <bool RAW>
-__device__ void pass_sigprop(const BlockSmem &b, int stripes, int p, int band, Mq &mq, Raw &raw, const T1Tables &T,
-                             int lane) {
-  const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
-  for (int s = 0; s < stripes; ++s) {
-    uint32_t *row = cword(b, s, 0);
-    for (int c0 = 0; c0 < b.w; c0 += 32) {
-      // columns with a non-zero word; a sample that becomes significant gives the next
-      // column a significant neighbour, so that column joins the set (columns further
-      // right and the next chunk are unaffected or re-read from memory)
-      __syncwarp();
-      int c = c0 + lane;
-      uint32_t live = __ballot_sync(0xffffffffu, c < b.w && row[c] != 0);
-      while (live) {
-        int bit = __ffs(live) - 1;
-        live &= live - 1;
-        int col = c0 + bit;
-        uint32_t *wp = row + col;
-        uint32_t cw = *wp;
-        bool newsig = false;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if ((cw & ROW_NBR(k)) && !(cw & (ROW_SIG(k) | ROW_CHI(k)))) {
-            int sym = RAW ? raw_bit(raw) : mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
-            cw |= ROW_PI(k);
-            if (sym) {
-              int sg = decode_sign<RAW>(b, wp, cw, k, mq, raw, T);
-              b.sp.set_sig(4 * s + k, col, sg, p);
-              newsig = true;
-            }
-          }
-        }
-        *wp = cw;
-        if (newsig && bit < 31 && col + 1 < b.w) live |= 1u << (bit + 1);
-      }
+enum { P_SIGPROP = 0, P_MAGREF = 1, P_CLEANUP = 2 };
+
+// one decision: a raw bit in a bypass segment, else an MQ symbol
+__device__ __forceinline__ int decide(bool israw, Raw &raw, Mq &mq, uint2 *slot, const uint2 *tab) {
+  return israw ? raw_bit(raw) : mq_decode(mq, slot, tab);
+}
+
+// Sign of row k (raw bit, or MQ symbol in the sign context of its neighbours XOR the
+// context's prediction bit), then the sample becomes significant
+__device__ __forceinline__ void significant(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int k, int col,
+                                            int p, bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
+  int flip = 0, slot = C_SIGN;
+  if (!israw) {
+    const int sv = T.sc[sign_index(cw, wp[-1], wp[1], k)];
+    slot += sv >> 1;
+    flip = sv & 1;
+  }
+  const int sg = decide(israw, raw, mq, b.cx + slot, T.mq) ^ flip;
+  spread_sig(b, wp, cw, k, sg);
+  b.sp.set_sig(row + k, col, sg, p);
+}
+
+// significance propagation of one stripe column (bmi_block_decoder.cpp:10-215): rows
+// not yet significant with a significant neighbour
+__device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int col, int p,
+                                               bool israw, const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
+  bool newsig = false;
+#pragma unroll 1
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t v = cw >> (3 * k);
+    if (!(v & NBR_ROW0) || (v & (0x10u | (1u << CHI_POS)))) continue;
+    const int d = decide(israw, raw, mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq);
+    cw |= ROW_PI(k);
+    if (d) {
+      significant(b, wp, cw, row, k, col, p, israw, raw, mq, T);
+      newsig = true;
     }
   }
+  return newsig;
 }
 
-// magnitude refinement (bmi_block_decoder.cpp:217-349)
-template <bool RAW>
-__device__ void pass_magref(const BlockSmem &b, int stripes, int p, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
+// magnitude refinement of one stripe column (bmi_block_decoder.cpp:217-349)
+__device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, uint8_t *rf, int row, int col, int p,
+                                              bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
+  const uint32_t refined = *rf;
+  uint32_t now = 0;
+#pragma unroll 1
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t v = cw >> (3 * k);
+    if ((v & (0x10u | (1u << MU_POS))) != (0x10u | (1u << MU_POS))) continue;
+    // first refinement of this sample <=> (|v| >> p) < 4 in the reference
+    const int ctx = C_MAG + (((refined >> k) & 1) ? 2 : ((v & NBR_ROW0) ? 1 : 0));
+    const int d = decide(israw, raw, mq, b.cx + ctx, T.mq);
+    b.sp.refine(row + k, col, d, p);
+    now |= 1u << k;
+  }
+  if (now) *rf = (uint8_t)(refined | now);
+}
+
+// cleanup of one stripe column (bmi_block_decoder.cpp:351-586): an all-zero column is
+// coded in run mode (one run-length symbol; if it is 1, two uniform symbols give the row
+// of the first significant sample, whose sign follows directly); then every row not yet
+// coded in this bit-plane
+__device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int col, int p,
+                                               const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
+  int k = 0;
+  bool forced = false;
+  if (cw == 0) {
+    // run-length symbol, then the two uniform symbols (the reference's fixed-Qe
+    // MQ_DECODE_START is an ordinary decision on a context pinned at state 46)
+    int r = 0;
+#pragma unroll 1
+    for (int i = 0; i < 3; ++i) {
+      const int d = mq_decode(mq, b.cx + (i == 0 ? C_RUN : C_UNI), T.mq);
+      if (i == 0 && !d) return false;  // the whole column stays insignificant
+      r = (r << 1) | d;
+    }
+    k = r & 3;
+    forced = true;
+  }
+  bool newsig = false;
+#pragma unroll 1
+  for (; k < 4; ++k) {
+    if (!forced) {
+      const uint32_t v = cw >> (3 * k);
+      if (v & (0x10u | (1u << CHI_POS) | (1u << PI_POS))) continue;
+      if (!mq_decode(mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq)) continue;
+    }
+    forced = false;
+    significant(b, wp, cw, row, k, col, p, false, raw, mq, T);
+    newsig = true;
+  }
+  cw |= (cw << (MU_POS - 4)) & MU_ALL;
+  cw &= ~PI_ALL;
+  return newsig;
+}
+
+// One coding pass over the block.  Columns are visited in 32-column chunks: a ballot
+// selects the columns with work (non-zero word for significance propagation, a refinable
+// sample for refinement, every column for cleanup); a sample that becomes significant makes
+// the next column non-zero, so that column joins the set.  In cleanup, a run of all-zero
+// columns whose run-length symbols would all decode as MPS without renormalisation
+// (C >= k*Qe and A - k*Qe >= 0x8000, scaled) is consumed in one step: A -= k*Qe, C -= k*Qe.
+// Each pass inlines its decision sites once, without unrolling over the four rows, so the
+// kernel stays small enough for the instruction cache when many warps are resident.
+__device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p, int pass, bool israw,
+                                         const uint8_t *zc, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
   for (int s = 0; s < stripes; ++s) {
     uint32_t *row = cword(b, s, 0);
     uint8_t *rrow = b.rf + s * b.gap;
     for (int c0 = 0; c0 < b.w; c0 += 32) {
       __syncwarp();
-      int c = c0 + lane;
-      uint32_t live = __ballot_sync(0xffffffffu, c < b.w && (row[c] & MU_ALL) != 0);
+      const int c = c0 + lane;
+      const bool valid = c < b.w;
+      const uint32_t word = valid ? row[c] : 0u;
+      const bool work = pass == P_SIGPROP ? word != 0 : (pass == P_MAGREF ? (word & MU_ALL) != 0 : true);
+      uint32_t live = __ballot_sync(0xffffffffu, valid && work);
+      uint32_t zero = __ballot_sync(0xffffffffu, valid && word == 0);
       while (live) {
-        int bit = __ffs(live) - 1;
-        live &= live - 1;
-        int col = c0 + bit;
-        uint32_t cw = row[col];
-        uint32_t refined = rrow[col], now = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          if ((cw & (ROW_MU(k) | ROW_SIG(k))) == (ROW_MU(k) | ROW_SIG(k))) {
-            int sym;
-            if (RAW) {
-              sym = raw_bit(raw);
-            } else {
-              // first refinement of this sample <=> (|v| >> p) < 4 in the reference
-              int ctx = C_MAG;
-              if (!((refined >> k) & 1)) {
-                if (cw & ROW_NBR(k)) ctx++;
-              } else {
-                ctx += 2;
-              }
-              sym = mq_decode(mq, b.cx + ctx, T.mq);
-            }
-            b.sp.refine(4 * s + k, col, sym, p);
-            now |= 1u << k;
-          }
-        }
-        rrow[col] = (uint8_t)(refined | now);
-      }
-    }
-  }
-}
-
-// number of consecutive zero context words in row[col, w), counted up to `limit`
-__device__ __forceinline__ int zero_run(const uint32_t *row, int col, int w, int limit, int lane) {
-  int run = 0;
-  while (run < limit && col + run < w) {
-    const int c = col + run + lane;
-    const uint32_t nz = __ballot_sync(0xffffffffu, c >= w || row[c] != 0);
-    if (nz) return min(limit, run + __ffs(nz) - 1);
-    run += 32;
-  }
-  return min(limit, run);
-}
-
-// cleanup with run mode (bmi_block_decoder.cpp:351-586)
-__device__ void pass_cleanup(const BlockSmem &b, int stripes, int p, int band, Mq &mq, const T1Tables &T,
-                             int lane) {
-  const uint8_t *zc = T.zc[band == 3 ? 2 : (band == 1 ? 1 : 0)];
-  Raw dummy;
-  for (int s = 0; s < stripes; ++s) {
-    uint32_t *row = cword(b, s, 0);
-    __syncwarp();
-    for (int col = 0; col < b.w; ++col) {
-      uint32_t *wp = row + col;
-      uint32_t cw = *wp;
-      int k0 = 0;
-      if (cw == 0) {
-        // run of columns whose run-length symbols are MPS (0) without renormalisation
-        const uint2 e = b.cx[C_RUN];
-        if (!((e.y >> 16) & 1)) {
+        const int bit = __ffs(live) - 1;
+        if (pass == P_CLEANUP && ((zero >> bit) & 1)) {
+          const uint2 e = b.cx[C_RUN];
           const int32_t q = (int32_t)e.x;
-          const int32_t room = mq.A - 0x800000;
-          if (room >= q && mq.C >= q) {
-            const int lim = min(room / q, mq.C / q);
-            __syncwarp();
-            const int k = zero_run(row, col, b.w, lim, lane);
-            if (k > 0) {
-              mq.A -= k * q;
-              mq.C -= k * q;
-              col += k - 1;
-              continue;
-            }
+          const int32_t m = min(mq.A - 0x800000, mq.C);
+          if (!((e.y >> 16) & 1) && m >= q) {
+            int n = __clz(__brev(~(zero >> bit)));  // zero columns from `bit` on, in this chunk
+            if (n * q > m) n = m / q;
+            mq.A -= n * q;
+            mq.C -= n * q;
+            const uint32_t span = n >= 32 ? 0xffffffffu : ((1u << n) - 1u);
+            live &= ~(span << bit);
+            continue;
           }
         }
-        if (!mq_decode(mq, b.cx + C_RUN, T.mq)) continue;  // whole column stays insignificant
-        int r = mq_uniform(mq);
-        r = (r << 1) | mq_uniform(mq);
-        int sg = decode_sign<false>(b, wp, cw, r, mq, dummy, T);
-        b.sp.set_sig(4 * s + r, col, sg, p);
-        k0 = r + 1;
-      }
-      for (int k = k0; k < 4; ++k) {
-        if (cw & (ROW_SIG(k) | ROW_CHI(k) | ROW_PI(k))) continue;
-        int sym = mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
-        if (sym) {
-          int sg = decode_sign<false>(b, wp, cw, k, mq, dummy, T);
-          b.sp.set_sig(4 * s + k, col, sg, p);
+        live &= live - 1;
+        const int col = c0 + bit;
+        uint32_t *wp = row + col;
+        uint32_t cw = *wp;
+        if (pass == P_MAGREF) {
+          magref_column(b, cw, rrow + col, 4 * s, col, p, israw, raw, mq, T);
+          continue;
+        }
+        const bool newsig = pass == P_SIGPROP ? sigprop_column(b, wp, cw, 4 * s, col, p, israw, zc, raw, mq, T)
+                                              : cleanup_column(b, wp, cw, 4 * s, col, p, zc, raw, mq, T);
+        *wp = cw;
+        if (newsig && bit < 31) {
+          if (pass == P_SIGPROP) live |= 1u << (bit + 1);
+          zero &= ~(1u << (bit + 1));
         }
       }
-      cw |= (cw << (MU_POS - 4)) & MU_ALL;
-      cw &= ~PI_ALL;
-      *wp = cw;
     }
   }
   __syncwarp();
@@ -439,6 +445,7 @@ __device__ __forceinline__ void init_states(uint2 *cx, const uint2 *tab) {
   for (int i = 0; i < N_CTX; ++i) cx[i] = tab[0];
   cx[C_SIG] = tab[4 << 1];
   cx[C_RUN] = tab[3 << 1];
+  cx[C_UNI] = tab[46 << 1];
 }
 
 __device__ __forceinline__ bool seg_starts(int flags, int j) {
@@ -465,16 +472,14 @@ __device__ __forceinline__ void block_planes(const j2k_cblk &cb, int &bit_plane,
 }
 
 // Decode one code-block with the whole warp.  Returns a status (0 ok).
-__device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens,
+__device__ __forceinline__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens,
                             const BlockSmem &b, const T1Tables &T, int lane, int bit_plane, int num_passes) {
   const int w = cb.w, h = cb.h;
   const int stripes = (h + 3) >> 2;
   // clear the block's samples (output region), context words and refinement bits; mark
   // OOB columns and a partial last stripe
-  for (int i = lane; i < w * h; i += 32) {
-    const int y = i / w, x = i - y * w;
-    b.sp.base[(size_t)y * b.sp.stride + x] = 0;
-  }
+  for (int y = 0; y < h; ++y)
+    for (int x = lane; x < w; x += 32) b.sp.base[(size_t)y * b.sp.stride + x] = 0;
   const int nwords = (stripes + 2) * b.gap + 2;
   for (int i = lane; i < nwords; i += 32) b.cw[i] = 0;
   for (int i = lane; i < stripes * b.gap; i += 32) b.rf[i] = 0;
@@ -497,12 +502,13 @@ __device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ byte
   if (num_passes > 0 && 30 - (int)cb.missing <= 0) return 1;
 
   const int multi = (cb.flags & (J2K_CB_BYPASS | J2K_CB_TERMALL)) != 0;
+  const uint8_t *zc = T.zc[cb.band == 3 ? 2 : (cb.band == 1 ? 1 : 0)];
   const uint8_t *data = bytes + cb.data_off;
   Mq mq;
   Raw raw;
   mq.A = mq.C = mq.t = mq.T = 0;
-  mq.pos = mq.end = 0;
-  mq.base = data;
+  mq.ap = mq.aend = mq.cur = mq.nxt = 0;
+  mq.w = reinterpret_cast<const uint32_t *>(bytes);
   raw_init(raw, data, 0);
   uint32_t seg_pos = 0;
   int seg_idx = 0;
@@ -538,17 +544,9 @@ __device__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ byte
       else mq_init(mq, data + seg_pos, len);
       seg_pos += len;
     }
-    if (type == 0) {
-      if (israw) pass_sigprop<true>(b, stripes, bit_plane, cb.band, mq, raw, T, lane);
-      else pass_sigprop<false>(b, stripes, bit_plane, cb.band, mq, raw, T, lane);
-    } else if (type == 1) {
-      if (israw) pass_magref<true>(b, stripes, bit_plane, mq, raw, T, lane);
-      else pass_magref<false>(b, stripes, bit_plane, mq, raw, T, lane);
-    } else {
-      pass_cleanup(b, stripes, bit_plane, cb.band, mq, T, lane);
-      if (cb.flags & J2K_CB_SEGSYM)
-        for (int i = 0; i < 4; ++i) mq_uniform(mq);
-    }
+    run_pass(b, stripes, bit_plane, type, israw, zc, mq, raw, T, lane);
+    if (type == 2 && (cb.flags & J2K_CB_SEGSYM))
+      for (int i = 0; i < 4; ++i) mq_uniform(mq);
     if (cb.flags & J2K_CB_RESET) {
       __syncwarp();
       if (lane == 0) init_states(b.cx, T.mq);
