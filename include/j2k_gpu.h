@@ -130,6 +130,8 @@ typedef struct j2k_gpu_tuning {
   int t1_warps_per_cta;  /* code-blocks decoded concurrently per CTA */
   int dwt_tile;          /* output tile edge of the fused DWT kernels (32 or 64) */
   int use_graph;         /* capture Tier-1 + DWT launches of a batch into a CUDA graph */
+  int t1_form;           /* Tier-1 kernel form: 0 auto, 1 compact (throughput), 2 unrolled (latency) */
+  int t1_latency_waves;  /* auto form: unrolled while code-blocks <= this many x 32 warps x SMs */
 } j2k_gpu_tuning;
 int j2k_gpu_set_tuning(j2k_gpu_ctx *ctx, const j2k_gpu_tuning *t);
 int j2k_gpu_get_tuning(const j2k_gpu_ctx *ctx, j2k_gpu_tuning *t);

@@ -58,7 +58,7 @@ struct T1Layout {
 // Host-side queue classes: code-block size bound
 enum { Q64 = 0, Q32 = 1, NQ = 2 };
 
-template <int MAXW, int MAXH>
+template <int MAXW, int MAXH, bool UNROLLED>
 __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order,
                                                  int n, int *__restrict__ counter, const uint8_t *__restrict__ bytes,
                                                  const uint32_t *__restrict__ seglens, void *__restrict__ coef,
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cb
     if (cb.w == 0 || cb.h == 0 || cb.w > MAXW || cb.h > MAXH) {
       st = 9;
     } else {
-      st = decode_block(cb, bytes, seglens, b, T, lane, bit_plane, num_passes);
+      st = decode_block<UNROLLED>(cb, bytes, seglens, b, T, lane, bit_plane, num_passes);
     }
     // rewrite the block in place: raw sign-magnitude -> dequantised float (9/7) or shifted
     // integer (5/3); lane 0's atomic updates are made visible first
@@ -219,7 +219,7 @@ struct j2k_gpu_ctx {
   cudaEvent_t ev[6] = {};
   float t_t1 = 0, t_dwt = 0, t_h2d = 0, t_total = 0;
   int launches = 0;
-  j2k_gpu_tuning tuning{8, 64, 0};
+  j2k_gpu_tuning tuning{8, 64, 0, 0, 2};
   int sm_count = 148;
   size_t smem_optin = 227 * 1024;
 };
@@ -302,8 +302,10 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
     return J2K_ERR_CUDA;
   }
   // opt into the large dynamic shared memory of the Tier-1 kernels
-  cudaFuncSetAttribute(t1_kernel<64, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<32, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<32, 32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<32, 32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   *out = c;
   return J2K_OK;
 }
@@ -338,6 +340,8 @@ extern "C" int j2k_gpu_set_tuning(j2k_gpu_ctx *c, const j2k_gpu_tuning *t) {
   if (n.t1_warps_per_cta <= 0) n.t1_warps_per_cta = 8;
   if (n.t1_warps_per_cta > 32) n.t1_warps_per_cta = 32;
   if (n.dwt_tile <= 0) n.dwt_tile = 64;
+  if (n.t1_form < 0 || n.t1_form > 2) n.t1_form = 0;
+  if (n.t1_latency_waves <= 0) n.t1_latency_waves = 2;
   c->tuning = n;
   return J2K_OK;
 }
@@ -407,9 +411,9 @@ extern "C" int j2k_gpu_batch_footprint(const j2k_gpu_ctx *cc, size_t *bytes) {
 namespace {
 // Persistent Tier-1 launch: the CTA shape with the most resident warps per SM (registers,
 // shared memory and thread limits from the occupancy calculator), one wave of CTAs.
-template <int MAXW, int MAXH>
-void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
-               const uint32_t *seg, const T1Tables *tab) {
+template <int MAXW, int MAXH, bool UNROLLED>
+void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
+                  const uint32_t *seg, const T1Tables *tab) {
   typedef T1Layout<MAXW, MAXH> Lay;
   const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
   int best_w = 1, best_ctas = 1, best_warps = 0;
@@ -418,7 +422,8 @@ void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, cons
     const size_t sm = tsz + (size_t)w * Lay::PER_WARP;
     if (sm > c->smem_optin) break;
     int ctas = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH>, w * 32, sm) != cudaSuccess) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH, UNROLLED>, w * 32, sm) !=
+        cudaSuccess) {
       cudaGetLastError();
       continue;
     }
@@ -430,8 +435,27 @@ void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, cons
   }
   const size_t sm = tsz + (size_t)best_w * Lay::PER_WARP;
   const int grid = std::max(1, std::min((n + best_w - 1) / best_w, c->sm_count * std::max(1, best_ctas)));
-  t1_kernel<MAXW, MAXH><<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
-                                                           c->d_A.p, (uint16_t *)c->d_status.p, tab);
+  t1_kernel<MAXW, MAXH, UNROLLED><<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
+                                                                     c->d_A.p, (uint16_t *)c->d_status.p, tab);
+}
+
+// Kernel form: the unrolled (latency) form while the queue holds at most
+// `t1_latency_waves` blocks per resident warp slot of the GPU (the launch's time is then the
+// serial time of its longest blocks), the compact (throughput) form for longer queues.
+template <int MAXW, int MAXH>
+void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
+               const uint32_t *seg, const T1Tables *tab) {
+  bool unrolled;
+  if (c->tuning.t1_form == 1) {
+    unrolled = false;
+  } else if (c->tuning.t1_form == 2) {
+    unrolled = true;
+  } else {
+    const int waves = c->tuning.t1_latency_waves > 0 ? c->tuning.t1_latency_waves : 2;
+    unrolled = (long long)n <= (long long)waves * c->sm_count * 32;
+  }
+  if (unrolled) launch_t1_as<MAXW, MAXH, true>(c, st, n, cbs, ord, cnt, seg, tab);
+  else launch_t1_as<MAXW, MAXH, false>(c, st, n, cbs, ord, cnt, seg, tab);
 }
 }  // namespace
 

@@ -307,51 +307,97 @@ __device__ __forceinline__ void significant(const BlockSmem &b, uint32_t *wp, ui
   b.sp.set_sig(row + k, col, sg, p);
 }
 
+// Rows of a stripe column that pass a pass's test, as a 4-bit mask (bit k = row k), with
+// v = word >> 3k holding row k's bits at row 0's positions:
+// (v & FORBID) == 0 && (v & NEED) == NEED && (ANY == 0 || (v & ANY) != 0)
+template <uint32_t FORBID, uint32_t NEED, uint32_t ANY>
+__device__ __forceinline__ uint32_t row_mask(uint32_t cw) {
+  uint32_t m = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t v = cw >> (3 * k);
+    const bool ok = !(v & FORBID) && (v & NEED) == NEED && (ANY == 0 || (v & ANY) != 0);
+    m |= (uint32_t)ok << k;
+  }
+  return m;
+}
+constexpr uint32_t V_SIG = 0x10u, V_CHI = 1u << CHI_POS, V_MU = 1u << MU_POS, V_PI = 1u << PI_POS;
+
+// Two forms of each pass's column code, with identical decisions:
+//   UNROLLED = false (throughput): the rows to visit are a 4-bit mask walked with ffs, and
+//     each decision is inlined once, so the kernel stays small for the instruction cache
+//     when many warps are resident and sit in different passes;
+//   UNROLLED = true (latency): the four rows are unrolled with constant masks, trading
+//     code size for a shorter dependency chain per symbol, for batches too small to fill
+//     the GPU, whose time is the serial time of their longest blocks.
+
 // significance propagation of one stripe column (bmi_block_decoder.cpp:10-215): rows
-// not yet significant with a significant neighbour
+// not yet significant with a significant neighbour; a row that becomes significant can
+// make the rows below it eligible
+template <bool UNROLLED>
 __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int col, int p,
                                                bool israw, const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
   bool newsig = false;
-#pragma unroll 1
-  for (int k = 0; k < 4; ++k) {
-    const uint32_t v = cw >> (3 * k);
-    if (!(v & NBR_ROW0) || (v & (0x10u | (1u << CHI_POS)))) continue;
-    const int d = decide(israw, raw, mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq);
-    cw |= ROW_PI(k);
-    if (d) {
-      significant(b, wp, cw, row, k, col, p, israw, raw, mq, T);
-      newsig = true;
+  if constexpr (UNROLLED) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const uint32_t v = cw >> (3 * k);
+      if (!(v & NBR_ROW0) || (v & (V_SIG | V_CHI))) continue;
+      const int d = decide(israw, raw, mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq);
+      cw |= ROW_PI(k);
+      if (d) {
+        significant(b, wp, cw, row, k, col, p, israw, raw, mq, T);
+        newsig = true;
+      }
+    }
+  } else {
+    uint32_t todo = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw);
+    while (todo) {
+      const int k = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int d = decide(israw, raw, mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
+      cw |= ROW_PI(k);
+      if (d) {
+        significant(b, wp, cw, row, k, col, p, israw, raw, mq, T);
+        newsig = true;
+        todo = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw) & (0xEu << k);
+      }
     }
   }
   return newsig;
 }
 
-// magnitude refinement of one stripe column (bmi_block_decoder.cpp:217-349)
+// magnitude refinement of one stripe column (bmi_block_decoder.cpp:217-349): rows
+// significant before this bit-plane
+template <bool UNROLLED>
 __device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, uint8_t *rf, int row, int col, int p,
                                               bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
   const uint32_t refined = *rf;
-  uint32_t now = 0;
-#pragma unroll 1
-  for (int k = 0; k < 4; ++k) {
-    const uint32_t v = cw >> (3 * k);
-    if ((v & (0x10u | (1u << MU_POS))) != (0x10u | (1u << MU_POS))) continue;
-    // first refinement of this sample <=> (|v| >> p) < 4 in the reference
-    const int ctx = C_MAG + (((refined >> k) & 1) ? 2 : ((v & NBR_ROW0) ? 1 : 0));
-    const int d = decide(israw, raw, mq, b.cx + ctx, T.mq);
-    b.sp.refine(row + k, col, d, p);
-    now |= 1u << k;
+  const uint32_t rows = row_mask<0u, V_SIG | V_MU, 0u>(cw);
+#pragma unroll
+  for (int i = 0; i < (UNROLLED ? 4 : 1); ++i) {
+    uint32_t todo = UNROLLED ? (rows & (1u << i)) : rows;
+    while (todo) {
+      const int k = UNROLLED ? i : __ffs(todo) - 1;
+      todo &= todo - 1;
+      // first refinement of this sample <=> (|v| >> p) < 4 in the reference
+      const int ctx = C_MAG + (((refined >> k) & 1) ? 2 : (((cw >> (3 * k)) & NBR_ROW0) ? 1 : 0));
+      const int d = decide(israw, raw, mq, b.cx + ctx, T.mq);
+      b.sp.refine(row + k, col, d, p);
+    }
   }
-  if (now) *rf = (uint8_t)(refined | now);
+  if (rows) *rf = (uint8_t)(refined | rows);
 }
 
 // cleanup of one stripe column (bmi_block_decoder.cpp:351-586): an all-zero column is
 // coded in run mode (one run-length symbol; if it is 1, two uniform symbols give the row
 // of the first significant sample, whose sign follows directly); then every row not yet
 // coded in this bit-plane
+template <bool UNROLLED>
 __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int col, int p,
                                                const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
-  int k = 0;
-  bool forced = false;
+  int forced = -1;
+  uint32_t todo;
   if (cw == 0) {
     // run-length symbol, then the two uniform symbols (the reference's fixed-Qe
     // MQ_DECODE_START is an ordinary decision on a context pinned at state 46)
@@ -362,20 +408,22 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
       if (i == 0 && !d) return false;  // the whole column stays insignificant
       r = (r << 1) | d;
     }
-    k = r & 3;
-    forced = true;
+    forced = r & 3;
+    todo = (0xFu << forced) & 0xFu;
+  } else {
+    todo = row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw);
   }
   bool newsig = false;
-#pragma unroll 1
-  for (; k < 4; ++k) {
-    if (!forced) {
-      const uint32_t v = cw >> (3 * k);
-      if (v & (0x10u | (1u << CHI_POS) | (1u << PI_POS))) continue;
-      if (!mq_decode(mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq)) continue;
+#pragma unroll
+  for (int i = 0; i < (UNROLLED ? 4 : 1); ++i) {
+    uint32_t rows = UNROLLED ? (todo & (1u << i)) : todo;
+    while (rows) {
+      const int k = UNROLLED ? i : __ffs(rows) - 1;
+      rows &= rows - 1;
+      if (k != forced && !mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq)) continue;
+      significant(b, wp, cw, row, k, col, p, false, raw, mq, T);
+      newsig = true;
     }
-    forced = false;
-    significant(b, wp, cw, row, k, col, p, false, raw, mq, T);
-    newsig = true;
   }
   cw |= (cw << (MU_POS - 4)) & MU_ALL;
   cw &= ~PI_ALL;
@@ -390,6 +438,7 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
 // (C >= k*Qe and A - k*Qe >= 0x8000, scaled) is consumed in one step: A -= k*Qe, C -= k*Qe.
 // Each pass inlines its decision sites once, without unrolling over the four rows, so the
 // kernel stays small enough for the instruction cache when many warps are resident.
+template <bool UNROLLED>
 __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p, int pass, bool israw,
                                          const uint8_t *zc, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
   for (int s = 0; s < stripes; ++s) {
@@ -424,11 +473,11 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
         uint32_t *wp = row + col;
         uint32_t cw = *wp;
         if (pass == P_MAGREF) {
-          magref_column(b, cw, rrow + col, 4 * s, col, p, israw, raw, mq, T);
+          magref_column<UNROLLED>(b, cw, rrow + col, 4 * s, col, p, israw, raw, mq, T);
           continue;
         }
-        const bool newsig = pass == P_SIGPROP ? sigprop_column(b, wp, cw, 4 * s, col, p, israw, zc, raw, mq, T)
-                                              : cleanup_column(b, wp, cw, 4 * s, col, p, zc, raw, mq, T);
+        const bool newsig = pass == P_SIGPROP ? sigprop_column<UNROLLED>(b, wp, cw, 4 * s, col, p, israw, zc, raw, mq, T)
+                                              : cleanup_column<UNROLLED>(b, wp, cw, 4 * s, col, p, zc, raw, mq, T);
         *wp = cw;
         if (newsig && bit < 31) {
           if (pass == P_SIGPROP) live |= 1u << (bit + 1);
@@ -472,6 +521,7 @@ __device__ __forceinline__ void block_planes(const j2k_cblk &cb, int &bit_plane,
 }
 
 // Decode one code-block with the whole warp.  Returns a status (0 ok).
+template <bool UNROLLED>
 __device__ __forceinline__ int decode_block(const j2k_cblk &cb, const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens,
                             const BlockSmem &b, const T1Tables &T, int lane, int bit_plane, int num_passes) {
   const int w = cb.w, h = cb.h;
@@ -544,7 +594,7 @@ __device__ __forceinline__ int decode_block(const j2k_cblk &cb, const uint8_t *_
       else mq_init(mq, data + seg_pos, len);
       seg_pos += len;
     }
-    run_pass(b, stripes, bit_plane, type, israw, zc, mq, raw, T, lane);
+    run_pass<UNROLLED>(b, stripes, bit_plane, type, israw, zc, mq, raw, T, lane);
     if (type == 2 && (cb.flags & J2K_CB_SEGSYM))
       for (int i = 0; i < 4; ++i) mq_uniform(mq);
     if (cb.flags & J2K_CB_RESET) {

@@ -64,7 +64,8 @@ class TileComp(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("t1_warps_per_cta", ctypes.c_int), ("dwt_tile", ctypes.c_int), ("use_graph", ctypes.c_int)]
+    _fields_ = [("t1_warps_per_cta", ctypes.c_int), ("dwt_tile", ctypes.c_int), ("use_graph", ctypes.c_int),
+                ("t1_form", ctypes.c_int), ("t1_latency_waves", ctypes.c_int)]
 
 
 class EncParams(ctypes.Structure):
@@ -350,8 +351,8 @@ class GpuContext:
         self._ck(lib().j2k_gpu_last_launches(self.h, ctypes.byref(n)), "last_launches")
         return n.value
 
-    def set_tuning(self, t1_warps_per_cta=0, dwt_tile=0, use_graph=0):
-        t = Tuning(t1_warps_per_cta, dwt_tile, use_graph)
+    def set_tuning(self, t1_warps_per_cta=0, dwt_tile=0, use_graph=0, t1_form=0, t1_latency_waves=0):
+        t = Tuning(t1_warps_per_cta, dwt_tile, use_graph, t1_form, t1_latency_waves)
         self._ck(lib().j2k_gpu_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def mem_usage(self):

@@ -43,8 +43,11 @@ def _decode_check(ctx, cs, fmt, flags=0):
 
 @pytest.mark.parametrize("name", sorted(n for n in os.listdir(GOLDEN) if n.endswith(".j2k")))
 @pytest.mark.parametrize("flags", [0, 1])
-def test_golden_streams_bit_exact(gpu_ctx, name, flags):
+@pytest.mark.parametrize("t1_form", [1, 2])
+def test_golden_streams_bit_exact(gpu_ctx, name, flags, t1_form):
+    """Both Tier-1 kernel forms (1 compact, 2 unrolled) on every fixture."""
     from jpeg2000_decoder_b200 import native
+    gpu_ctx.set_tuning(t1_form=t1_form)
     cs = _read(name)
     plan = native.Plan(cs)
     fmt = native.FMT_32BITS_4COMPONENTS if plan.info.ncomp == 1 else (
@@ -86,9 +89,11 @@ def test_c1_lossless_and_reference_rows(gpu_ctx):
     assert len(bad) == 31 and bad.min() == 481
 
 
-def test_c2_97_ict_1bpp_exact_and_fp64_budget(gpu_ctx):
-    """C2 at full size: 2048x2048 RGB, 9/7 + ICT at ~1 bpp."""
+@pytest.mark.parametrize("t1_form", [1, 2])
+def test_c2_97_ict_1bpp_exact_and_fp64_budget(gpu_ctx, t1_form):
+    """C2 at full size: 2048x2048 RGB, 9/7 + ICT at ~1 bpp, with both Tier-1 kernel forms."""
     from jpeg2000_decoder_b200 import native, synth
+    gpu_ctx.set_tuning(t1_form=t1_form)
     cs = synth.c2_stream(2)
     assert abs(len(cs) * 8 / (2048 * 2048) - 1.0) < 0.05
     out, plan = _decode_check(gpu_ctx, cs, native.FMT_24BITS_RGB)
