@@ -88,39 +88,56 @@ struct DwtTypes<false> {
   typedef float T;
 };
 
-// Lifting along one direction over the staged tile.  `horizontal` selects rows; positions
-// with both neighbours inside the 72-wide window are updated.
-template <bool REV, bool HORIZ>
-__device__ __forceinline__ void lift_tile(typename DwtTypes<REV>::T *t, int lines_begin, int lines_end) {
-  typedef typename DwtTypes<REV>::T T;
-  const int nl = lines_end - lines_begin;
-  const int half = (DWT_N - 2) / 2;  // 35 updates per parity per line
-  constexpr int NSTEP = REV ? 2 : 4;
-  const float coef[4] = {0.44350685204397f, 0.88291107553093f, -0.05298011857296f, -1.58613434205992f};
-#pragma unroll
-  for (int step = 0; step < NSTEP; ++step) {
-    const int parity = step & 1;  // even, odd, even, odd
-    for (int i = threadIdx.x; i < nl * half; i += blockDim.x) {
-      int line = lines_begin + i / half;
-      int pos = 2 - parity + 2 * (i % half);  // even: 2..70, odd: 1..69 (neighbours in [0, 72))
-      T *c, *l, *r;
-      if (HORIZ) {
-        c = t + line * DWT_PITCH + pos;
-        l = c - 1;
-        r = c + 1;
-      } else {
-        c = t + pos * DWT_PITCH + line;
-        l = c - DWT_PITCH;
-        r = c + DWT_PITCH;
-      }
-      if constexpr (REV) {
-        if (parity == 0) *c = *c - ((*l + *r + 2) >> 2);
-        else *c = *c + ((*l + *r) >> 1);
-      } else {
-        *c = lift97(*c, coef[step], *l, *r);
-      }
+constexpr int DWT_THREADS = 128;  // threads per CTA of the level kernels
+
+// Lifting of one window line (72 samples, element stride `st`), streamed by one thread
+// through registers: iteration m reads the pair (x[2m], x[2m+1]) and retires the samples
+// whose every lifting step is complete, in place behind the read position.  The values are
+// those of the step-by-step scheme that updates evens 2..70 and odds 1..69 in each step
+// (x[0] and x[71] keep their input values), which the 4-sample halo makes exact for the 64
+// centre positions; positions above 67 are not all written.
+template <bool REV>
+__device__ __forceinline__ void lift_line(typename DwtTypes<REV>::T *p, int st) {
+  constexpr int NP = DWT_N / 2;  // 36 pairs
+  if constexpr (REV) {
+    // x[2n] -= (x[2n-1] + x[2n+1] + 2) >> 2; x[2n+1] += (x[2n] + x[2n+2]) >> 1
+    int xo_prev = p[st], e_prev = p[0];  // pair 0: x[0] is not updated
+#pragma unroll 5
+    for (int m = 1; m < NP; ++m) {
+      const int xe = p[2 * m * st], xo = p[(2 * m + 1) * st];
+      const int e = xe - ((xo_prev + xo + 2) >> 2);
+      const int o = xo_prev + ((e_prev + e) >> 1);  // position 2m-1
+      p[2 * m * st] = e;
+      p[(2 * m - 1) * st] = o;
+      xo_prev = xo;
+      e_prev = e;
     }
-    __syncthreads();
+  } else {
+    // steps c0 (evens), c1 (odds), c2 (evens), c3 (odds): x -= c * (left + right), each
+    // operation rounded separately
+    const float c0 = 0.44350685204397f, c1 = 0.88291107553093f, c2 = -0.05298011857296f, c3 = -1.58613434205992f;
+    const float x0 = p[0], x1 = p[st];
+    const float x2 = p[2 * st], x3 = p[3 * st];
+    // m = 1
+    float e0_prev = lift97(x2, c0, x1, x3);     // e0 at 2
+    float o1_prev = lift97(x1, c1, x0, e0_prev);  // o1 at 1 (e0 at 0 = x0)
+    float e2_prev = x0;                            // e2 at 0 = x0
+    float xo_prev = x3;
+    p[0] = x0;
+#pragma unroll 5
+    for (int m = 2; m < NP; ++m) {
+      const float xe = p[2 * m * st], xo = p[(2 * m + 1) * st];
+      const float e0 = lift97(xe, c0, xo_prev, xo);           // position 2m
+      const float o1 = lift97(xo_prev, c1, e0_prev, e0);      // position 2m-1
+      const float e2 = lift97(e0_prev, c2, o1_prev, o1);      // position 2m-2
+      const float o3 = lift97(o1_prev, c3, e2_prev, e2);      // position 2m-3
+      p[(2 * m - 2) * st] = e2;
+      p[(2 * m - 3) * st] = o3;
+      xo_prev = xo;
+      e0_prev = e0;
+      o1_prev = o1;
+      e2_prev = e2;
+    }
   }
 }
 
@@ -130,81 +147,119 @@ __device__ __forceinline__ typename DwtTypes<REV>::T *dwt_buf(int id, void *a, v
   return (T *)(id == 0 ? a : (id == 1 ? b : c));
 }
 
+// Shared memory of one CTA: the staged window, the reference-compat column-end inputs and
+// the source row / column of every window line (mirrored, low or high part)
 template <bool REV>
-__global__ void __launch_bounds__(256) dwt_level_kernel(const DwtLevel *__restrict__ levels,
-                                                        const DwtTask *__restrict__ tasks, int ntasks, void *bufA,
-                                                        void *bufB, void *bufC, float ll_gain_value) {
+struct DwtSmem {
+  typename DwtTypes<REV>::T tile[DWT_N * DWT_PITCH];
+  typename DwtTypes<REV>::T keep[2][DWT_T];
+  int32_t srow[DWT_N], scol[DWT_N];
+};
+
+// One 64x64 output tile of one level.  `quad`: the level's Mallat quadrants (LL taken from
+// `llsrc` instead, scaled by `gain` when ll_gain); output to `out`.
+template <bool REV>
+__device__ __forceinline__ void dwt_tile(DwtSmem<REV> &S, const typename DwtTypes<REV>::T *quad, int stride_q,
+                                         const typename DwtTypes<REV>::T *llsrc, int stride_ll,
+                                         typename DwtTypes<REV>::T *out, int stride_out, int rw, int rh, int lw,
+                                         int lh, bool ll_gain, float gain, bool refcompat, int ox, int oy) {
   typedef typename DwtTypes<REV>::T T;
-  __shared__ T tile[DWT_N * DWT_PITCH];
-  __shared__ T keep[2][DWT_T];  // reference-compat inputs of the column end
-  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
-    const DwtTask tk = tasks[task];
-    const DwtLevel L = levels[tk.level];
-    const int ox = tk.tx * DWT_T, oy = tk.ty * DWT_T;
-    const T *A = dwt_buf<REV>(0, bufA, bufB, bufC) + L.base;
-    const T *LLsrc = dwt_buf<REV>(L.ll_src, bufA, bufB, bufC) + L.base;
-    T *out = dwt_buf<REV>(L.out_dst, bufA, bufB, bufC) + L.base;
-    // ---- stage the interleaved window with a mirrored halo
-    for (int i = threadIdx.x; i < DWT_N * DWT_N; i += blockDim.x) {
-      const int iy = i / DWT_N, ix = i % DWT_N;
-      const int y = mirror(oy - DWT_H + iy, L.rh);
-      const int x = mirror(ox - DWT_H + ix, L.rw);
-      const int sy = (y & 1) ? L.lh + (y >> 1) : (y >> 1);
-      const int sx = (x & 1) ? L.lw + (x >> 1) : (x >> 1);
-      T v;
-      if (!(x & 1) && !(y & 1)) {
-        v = LLsrc[(size_t)sy * L.stride + sx];
-        if (!REV && L.ll_gain) v = (T)__fmul_rn((float)v, ll_gain_value);
-      } else {
-        v = A[(size_t)sy * L.stride + sx];
-      }
-      tile[iy * DWT_PITCH + ix] = v;
+  T *tile = S.tile;
+  // source line of every window row / column: window index i <-> position o - 4 + i, whose
+  // mirror keeps its parity, so even window lines come from the low part and odd ones
+  // from the high part
+  for (int i = threadIdx.x; i < 2 * DWT_N; i += blockDim.x) {
+    const bool col = i >= DWT_N;
+    const int w = col ? i - DWT_N : i;
+    const int n = col ? rw : rh, lo = col ? lw : lh;
+    // the window may reach far past a level smaller than the tile: full periodic mirror
+    const int x = mirror((col ? ox : oy) - DWT_H + w, n);
+    const int src = (x & 1) ? lo + (x >> 1) : (x >> 1);
+    if (col) S.scol[w] = src;
+    else S.srow[w] = src;
+  }
+  __syncthreads();
+  // stage quadrant by quadrant: consecutive threads read consecutive source columns
+  constexpr int QN = DWT_N / 2;  // 36 window lines of each parity
+  for (int e = threadIdx.x; e < 4 * QN * QN; e += blockDim.x) {
+    const int qd = e / (QN * QN), r = (e - qd * QN * QN) / QN, j = e - qd * QN * QN - r * QN;
+    const int iy = 2 * r + (qd >> 1), ix = 2 * j + (qd & 1);
+    T v;
+    if (qd == 0) {
+      v = llsrc[(size_t)S.srow[iy] * stride_ll + S.scol[ix]];
+      if (!REV && ll_gain) v = (T)__fmul_rn((float)v, gain);
+    } else {
+      v = quad[(size_t)S.srow[iy] * stride_q + S.scol[ix]];
+    }
+    tile[iy * DWT_PITCH + ix] = v;
+  }
+  __syncthreads();
+  if (rw > 1) {
+    for (int r = threadIdx.x; r < DWT_N; r += blockDim.x) lift_line<REV>(tile + r * DWT_PITCH, 1);
+    __syncthreads();
+  }
+  // reference-compat: keep the horizontally transformed inputs the column end reads
+  const int n = rh;
+  const bool fix = REV && refcompat && n >= 3 && (oy <= n - 1) && (n - 2 < oy + DWT_T);
+  if (fix) {
+    int rowA, rowB = -1;
+    if (!(n & 1)) {
+      rowA = n - 3;  // H[m-2]
+    } else {
+      const int m = (n + 1) / 2;
+      rowA = n - 3;                 // L[m-2]
+      rowB = (m >= 3) ? n - 4 : 1;  // H[m-3] (H[0] when m == 2)
+    }
+    for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
+      S.keep[0][c] = tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+      if (rowB >= 0) S.keep[1][c] = tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
     }
     __syncthreads();
-    if (L.rw > 1) lift_tile<REV, true>(tile, 0, DWT_N);
-    // reference-compat: keep the horizontally transformed inputs the column end reads
-    const int n = L.rh;
-    const bool fix = REV && L.refcompat && n >= 3 && (oy <= n - 1) && (n - 2 < oy + DWT_T);
-    int rowA = -1, rowB = -1;
+  }
+  if (rh > 1) {
+    for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) lift_line<REV>(tile + DWT_H + c, DWT_PITCH);
+    __syncthreads();
+  }
+  if constexpr (REV) {
     if (fix) {
-      if (!(n & 1)) {
-        rowA = n - 3;  // H[m-2]
-      } else {
-        const int m = (n + 1) / 2;
-        rowA = n - 3;                    // L[m-2]
-        rowB = (m >= 3) ? n - 4 : 1;     // H[m-3] (H[0] when m == 2)
-      }
-      for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
-        keep[0][c] = tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
-        if (rowB >= 0) keep[1][c] = tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
-      }
-      __syncthreads();
-    }
-    if (L.rh > 1) lift_tile<REV, false>(tile, DWT_H, DWT_H + DWT_T);
-    if constexpr (REV) {
-      if (fix) {
       for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
         T *col = tile + DWT_H + c;
         const int r1 = n - 1 - oy + DWT_H, r2 = n - 2 - oy + DWT_H, r3 = n - 3 - oy + DWT_H;
         if (!(n & 1)) {
-          col[r1 * DWT_PITCH] = keep[0][c] + col[r2 * DWT_PITCH];
+          col[r1 * DWT_PITCH] = S.keep[0][c] + col[r2 * DWT_PITCH];
         } else {
-          const T hx = keep[1][c];
-          const T x1 = keep[0][c] - ((hx + 1) >> 1);
+          const T hx = S.keep[1][c];
+          const T x1 = S.keep[0][c] - ((hx + 1) >> 1);
           col[r1 * DWT_PITCH] = x1;
           col[r2 * DWT_PITCH] = hx + ((x1 + col[r3 * DWT_PITCH]) >> 1);
         }
       }
       __syncthreads();
-      }
     }
-    // ---- write the 64x64 result
-    const int ow = min(DWT_T, L.rw - ox), oh = min(DWT_T, L.rh - oy);
-    for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
-      const int yy = i / DWT_T, xx = i % DWT_T;
-      if (yy < oh && xx < ow) out[(size_t)(oy + yy) * L.stride + ox + xx] = tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
-    }
-    __syncthreads();
+  }
+  // write the 64x64 result
+  const int ow = min(DWT_T, rw - ox), oh = min(DWT_T, rh - oy);
+  for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
+    const int yy = i / DWT_T, xx = i % DWT_T;
+    if (yy < oh && xx < ow) out[(size_t)(oy + yy) * stride_out + ox + xx] = tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
+  }
+  __syncthreads();
+}
+
+template <bool REV>
+__global__ void __launch_bounds__(DWT_THREADS) dwt_level_kernel(const DwtLevel *__restrict__ levels,
+                                                        const DwtTask *__restrict__ tasks, int ntasks, void *bufA,
+                                                        void *bufB, void *bufC, float ll_gain_value) {
+  typedef typename DwtTypes<REV>::T T;
+  __shared__ DwtSmem<REV> S;
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const DwtTask tk = tasks[task];
+    const DwtLevel L = levels[tk.level];
+    const T *A = dwt_buf<REV>(0, bufA, bufB, bufC) + L.base;
+    const T *LLsrc = dwt_buf<REV>(L.ll_src, bufA, bufB, bufC) + L.base;
+    T *out = dwt_buf<REV>(L.out_dst, bufA, bufB, bufC) + L.base;
+    dwt_tile<REV>(S, A, L.stride, LLsrc, L.stride, out, L.stride, L.rw, L.rh, L.lw, L.lh, L.ll_gain != 0,
+                  ll_gain_value, L.refcompat != 0, tk.tx * DWT_T, tk.ty * DWT_T);
   }
 }
 
@@ -325,72 +380,14 @@ namespace j2k_dev {
 // tables in device memory): the CTA index selects the 64x64 output tile.  Used by the
 // entry point that runs on a static scratch array (noalloc.cu).
 template <bool REV>
-__global__ void __launch_bounds__(256) dwt_level_explicit_kernel(
+__global__ void __launch_bounds__(DWT_THREADS) dwt_level_explicit_kernel(
     const typename DwtTypes<REV>::T *__restrict__ quad, int stride_q, const typename DwtTypes<REV>::T *llsrc,
     int stride_ll, typename DwtTypes<REV>::T *out, int stride_out, int rw, int rh, int lw, int lh, int ll_gain,
     float ll_gain_value, int refcompat) {
-  typedef typename DwtTypes<REV>::T T;
-  __shared__ T tile[DWT_N * DWT_PITCH];
-  __shared__ T keep[2][DWT_T];
+  __shared__ DwtSmem<REV> S;
   const int tiles_x = (rw + DWT_T - 1) / DWT_T;
-  const int ox = (blockIdx.x % tiles_x) * DWT_T, oy = (blockIdx.x / tiles_x) * DWT_T;
-  for (int i = threadIdx.x; i < DWT_N * DWT_N; i += blockDim.x) {
-    const int iy = i / DWT_N, ix = i % DWT_N;
-    const int y = mirror(oy - DWT_H + iy, rh);
-    const int x = mirror(ox - DWT_H + ix, rw);
-    const int sy = (y & 1) ? lh + (y >> 1) : (y >> 1);
-    const int sx = (x & 1) ? lw + (x >> 1) : (x >> 1);
-    T v;
-    if (!(x & 1) && !(y & 1)) {
-      v = llsrc[(size_t)sy * stride_ll + sx];
-      if (!REV && ll_gain) v = (T)__fmul_rn((float)v, ll_gain_value);
-    } else {
-      v = quad[(size_t)sy * stride_q + sx];
-    }
-    tile[iy * DWT_PITCH + ix] = v;
-  }
-  __syncthreads();
-  if (rw > 1) lift_tile<REV, true>(tile, 0, DWT_N);
-  const int n = rh;
-  const bool fix = REV && refcompat && n >= 3 && (oy <= n - 1) && (n - 2 < oy + DWT_T);
-  int rowA = -1, rowB = -1;
-  if (fix) {
-    if (!(n & 1)) {
-      rowA = n - 3;
-    } else {
-      const int m = (n + 1) / 2;
-      rowA = n - 3;
-      rowB = (m >= 3) ? n - 4 : 1;
-    }
-    for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
-      keep[0][c] = tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
-      if (rowB >= 0) keep[1][c] = tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
-    }
-    __syncthreads();
-  }
-  if (rh > 1) lift_tile<REV, false>(tile, DWT_H, DWT_H + DWT_T);
-  if constexpr (REV) {
-    if (fix) {
-      for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
-        T *col = tile + DWT_H + c;
-        const int r1 = n - 1 - oy + DWT_H, r2 = n - 2 - oy + DWT_H, r3 = n - 3 - oy + DWT_H;
-        if (!(n & 1)) {
-          col[r1 * DWT_PITCH] = keep[0][c] + col[r2 * DWT_PITCH];
-        } else {
-          const T hx = keep[1][c];
-          const T x1 = keep[0][c] - ((hx + 1) >> 1);
-          col[r1 * DWT_PITCH] = x1;
-          col[r2 * DWT_PITCH] = hx + ((x1 + col[r3 * DWT_PITCH]) >> 1);
-        }
-      }
-      __syncthreads();
-    }
-  }
-  const int ow = min(DWT_T, rw - ox), oh = min(DWT_T, rh - oy);
-  for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
-    const int yy = i / DWT_T, xx = i % DWT_T;
-    if (yy < oh && xx < ow) out[(size_t)(oy + yy) * stride_out + ox + xx] = tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
-  }
+  dwt_tile<REV>(S, quad, stride_q, llsrc, stride_ll, out, stride_out, rw, rh, lw, lh, ll_gain != 0, ll_gain_value,
+                refcompat != 0, (blockIdx.x % tiles_x) * DWT_T, (blockIdx.x / tiles_x) * DWT_T);
 }
 
 }  // namespace j2k_dev

@@ -712,17 +712,17 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   const DwtLevel *d_lev = (const DwtLevel *)(D + o_lev);
   const DwtTask *d_dtk = (const DwtTask *)(D + o_dtk);
   const float llg = j2k::irrev_ll_gain();
-  const int dwt_cap = c->sm_count * 8;
+  const int dwt_cap = c->sm_count * 32;  // grid-stride cap: about three waves of resident CTAs
   for (int s = 0; s < maxL; ++s) {
     int n_rev = (int)(dtask_off[2 * s + 1] - dtask_off[2 * s]);
     int n_irr = (int)(dtask_off[2 * s + 2] - dtask_off[2 * s + 1]);
     if (n_rev) {
-      dwt_level_kernel<true><<<std::min(n_rev, dwt_cap), 256, 0, st>>>(d_lev, d_dtk + dtask_off[2 * s], n_rev, c->d_A.p,
+      dwt_level_kernel<true><<<std::min(n_rev, dwt_cap), DWT_THREADS, 0, st>>>(d_lev, d_dtk + dtask_off[2 * s], n_rev, c->d_A.p,
                                                                         c->d_B.p, c->d_C.p, llg);
       c->launches++;
     }
     if (n_irr) {
-      dwt_level_kernel<false><<<std::min(n_irr, dwt_cap), 256, 0, st>>>(d_lev, d_dtk + dtask_off[2 * s + 1], n_irr,
+      dwt_level_kernel<false><<<std::min(n_irr, dwt_cap), DWT_THREADS, 0, st>>>(d_lev, d_dtk + dtask_off[2 * s + 1], n_irr,
                                                                          c->d_A.p, c->d_B.p, c->d_C.p, llg);
       c->launches++;
     }

@@ -74,7 +74,7 @@ int run_levels(const j2k_tilecomp &tc, int flags, const void *coef, void *out, i
     T *dst = r == L ? reinterpret_cast<T *>(out) : half[r & 1];
     const int stride_out = r == L ? out_stride : sw;
     const int tiles = ((rw + j2k_dev::DWT_T - 1) / j2k_dev::DWT_T) * ((rh + j2k_dev::DWT_T - 1) / j2k_dev::DWT_T);
-    j2k_dev::dwt_level_explicit_kernel<REV><<<tiles, 256, 0, st>>>(reinterpret_cast<const T *>(coef), tc.w, llsrc,
+    j2k_dev::dwt_level_explicit_kernel<REV><<<tiles, j2k_dev::DWT_THREADS, 0, st>>>(reinterpret_cast<const T *>(coef), tc.w, llsrc,
                                                                    stride_ll, dst, stride_out, rw, rh, lw, lh,
                                                                    (!REV && r > 1) ? 1 : 0, llg, refc);
   }
