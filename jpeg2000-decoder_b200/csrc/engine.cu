@@ -55,8 +55,10 @@ struct T1Layout {
   static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 8) + 15) & ~15;
 };
 
-// Host-side queue classes: code-block size bound
-enum { Q64 = 0, Q32 = 1, NQ = 2 };
+// Host-side queue classes: code-block size bound.  One class: with 64 registers per thread
+// the register file, not shared memory, limits resident warps, so smaller blocks gain
+// nothing from a smaller per-warp layout, and one launch has one tail instead of two.
+enum { Q64 = 0, NQ = 1 };
 
 template <int MAXW, int MAXH, bool UNROLLED>
 __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order,
@@ -211,7 +213,7 @@ struct j2k_gpu_ctx {
   bool launched = false, synced = false, staged = false;
   // staged batch (device-resident inputs) for batch_run
   struct Staged {
-    size_t nq[2] = {0, 0}, n_cblks = 0, n_otasks = 0;
+    size_t nq[NQ] = {0}, n_cblks = 0, n_otasks = 0;
     size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0;
     int maxL = 0;
     std::vector<uint32_t> dtask_off;
@@ -303,9 +305,7 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
   }
   // opt into the large dynamic shared memory of the Tier-1 kernels
   cudaFuncSetAttribute(t1_kernel<64, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<32, 32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   cudaFuncSetAttribute(t1_kernel<64, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<32, 32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   *out = c;
   return J2K_OK;
 }
@@ -494,8 +494,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       cb.out_off += im.coef_base;
       uint32_t idx = (uint32_t)cbs.size();
       cbs.push_back(cb);
-      if (cb.num_passes == 0 && !(cb.flags & J2K_CB_IRREV) && false) continue;
-      ordq[(cb.w <= 32 && cb.h <= 32) ? Q32 : Q64].push_back(idx);
+      ordq[Q64].push_back(idx);
     }
     seg.insert(seg.end(), p.seglens.begin(), p.seglens.end());
     byte_base += p.bytes.size();
@@ -699,8 +698,7 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   for (int q = 0; q < NQ; ++q) {
     const int n = (int)G.nq[q];
     if (n) {
-      if (q == Q64) launch_t1<64, 64>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab);
-      else launch_t1<32, 32>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab);
+      launch_t1<64, 64>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab);
       c->launches++;
     }
     qoff += G.nq[q];
