@@ -1,6 +1,6 @@
 """Throughput benchmark of the B200 JPEG 2000 Part-1 decode path.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3|c2|c4|c1] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3|c2|c4|c1|c5] [--impl ours|reference]
 
 Default workload (metric: Mpixel/s decoded, batched): the batched video-frame decode —
 64 frames of 1920x1080 RGB 8-bit, 9/7 + ICT, 512x512 tiles, 5 levels, 64x64 code-blocks,
@@ -12,7 +12,8 @@ encoded and each appears 4 times in the batch (identical decode work per copy).
 One step = one decode of the whole batch.  `value` times steps with the coded bytes and
 work lists resident in HBM (CUDA events on the launch stream, L2 flushed between steps);
 `e2e` times the public C-ABI path from host memory: host Tier-2 of every frame,
-pinned H2D, decode, D2H of every decoded picture.  Multi-GPU runs are replicas (each rank
+pinned H2D, decode, D2H of every decoded picture.  `--workload c5` runs the serving stream
+through the continuous-batching service instead (see run_serve).  Multi-GPU runs are replicas (each rank
 decodes its own copy of the batch; images are independent, no collective on the data path).
 """
 import argparse
@@ -128,7 +129,8 @@ def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
     plans = [native.Plan(s) for s in streams[:max(1, min(len(streams), threads))]]
 
     def one(p):
-        oracle_util.oracle_decode(p, fmt)
+        f = fmt if fmt is not None else (native.FMT_24BITS_RGB if p.info.bitdepth <= 8 else native.FMT_48BITS_RGB)
+        oracle_util.oracle_decode(p, f)
         return p.info.width * p.info.height
 
     with ThreadPoolExecutor(max_workers=threads) as ex:
@@ -297,12 +299,153 @@ def run_gpu(args, rank, world, dist):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------ serving (C5) -------
+def run_serve(args, rank, world, dist):
+    """C5: requests of mixed size / depth / wavelet through the continuous-batching service.
+
+    Phase 1 (throughput): the whole request stream is submitted at once from several
+    threads while client threads take and release each result; value = decoded Mpixel/s
+    over that wall time (codestreams in host memory, packed pixels back in host memory: an
+    end-to-end figure).  Phase 2 (latency):
+    Poisson arrivals at `--rate` requests/s (default 70% of the phase-1 request rate);
+    p50 / p99 are submit-to-result times.  The plain path decodes the same stream one
+    request per launch sequence on one context."""
+    import threading
+
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg, pool, _ = workload("c5", args.quick)
+    fmts = [synth.c5_format(cs) for cs in pool]
+    px_of = [native.Plan(cs).info.width * native.Plan(cs).info.height for cs in pool]
+    n_req = args.requests or (200 if args.quick else 2000)
+    rng = np.random.default_rng(5 + rank)
+    order = [int(i) for i in rng.integers(0, len(pool), n_req)]
+    total_px = sum(px_of[i] for i in order)
+
+    # ---- plain path: one request per launch sequence
+    ctx = native.GpuContext(dev)
+    for i in range(len(pool)):
+        ctx.decode(pool[i], fmts[i])
+    n_plain = min(n_req, 4 * len(pool))
+    t0 = time.perf_counter()
+    for i in order[:n_plain]:
+        _, rc, _, _ = ctx.decode(pool[i], fmts[i])
+        assert rc == native.J2K_OK
+    plain_s = time.perf_counter() - t0
+    plain = sum(px_of[i] for i in order[:n_plain]) / plain_s / 1e6
+    ctx.close()
+
+    srv = native.Server(device=dev, pipeline_depth=args.depth, max_batch_pixels=int(args.batch_mpix * 2 ** 20))
+
+    def serve_pass(idx, when=None):
+        """Submit idx (at times `when` after the start, else at once) from 8 threads while 4
+        client threads take each result (zero-copy view) in submission order and release
+        it.  Returns (wall seconds, failed requests)."""
+        ids = [None] * len(idx)
+        ready = [threading.Event() for _ in idx]
+        failed = [0]
+        t_start = time.perf_counter()
+
+        def submitter(k, nthreads):
+            for j in range(k, len(idx), nthreads):
+                if when is not None:
+                    dt = t_start + when[j] - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                ids[j] = srv.submit(pool[idx[j]], fmts[idx[j]])
+                ready[j].set()
+
+        def client(k, nthreads):
+            for j in range(k, len(idx), nthreads):
+                ready[j].wait()
+                rc, view = srv.view(ids[j])
+                if rc != native.J2K_OK or view is None:
+                    failed[0] += 1
+                srv.release(ids[j])
+
+        th = [threading.Thread(target=submitter, args=(k, 8)) for k in range(8)]
+        th += [threading.Thread(target=client, args=(k, 4)) for k in range(4)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        return time.perf_counter() - t_start, failed[0]
+
+    # ---- warm-up: the device pools and pinned buffers grow to their steady-state sizes
+    for _ in range(max(1, args.warmup)):
+        serve_pass(order)
+
+    # ---- phase 1: saturation
+    srv.reset_stats()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        sat_s, bad = serve_pass(order)
+        torch.cuda.synchronize()
+    st1 = srv.stats()
+    if dist:
+        t = torch.tensor([sat_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sat_s = float(t.item())
+    value = total_px * world / sat_s / 1e6
+
+    # ---- phase 2: Poisson arrivals
+    rate = args.rate or 0.7 * n_req / sat_s
+    gaps = rng.exponential(1.0 / rate, n_req)
+    when = np.cumsum(gaps) - gaps[0]
+    srv.reset_stats()
+    poisson_s, bad2 = serve_pass(order, when)
+    bad += bad2
+    st2 = srv.stats()
+    srv.close()
+    if rank != 0:
+        return
+    cpu_v, cores, sample = cpu_decode_sample(pool, None, budget_s=args.cpu_budget)
+    h2d = sum(len(pool[i]) for i in order)
+    cfg = dict(cfg)
+    cfg.update({"requests": n_req, "pipeline_depth": args.depth, "batch_mpix_cap": args.batch_mpix, "parallelism": "replicas x%d" % world,
+                "bad_requests": bad, "l2": "inputs differ per request; no flush"})
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": 1,
+            "warmup": args.warmup, "ms_per_step": round(sat_s * 1e3, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (9/7) / int32 (5/3)",
+            "data": "synthetic (seeded requests, project encoder)", "config": cfg,
+            "e2e": {"value": round(value, 2), "unit": "Mpixel/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(sum(native.Plan(pool[i]).output_bytes(fmts[i]) for i in order)),
+                    "includes": "submit (host Tier-2) + merged batches + D2H of every request, wall clock"},
+            "serving": {"saturation": {"mpix_s": round(value, 2), "requests_s": round(n_req / sat_s, 1),
+                                       "gpu_busy_ms": round(st1["gpu_ms"], 2), "wall_ms": round(sat_s * 1e3, 2),
+                                       "host_stage_ms": round(st1["stage_ms"], 2),
+                                       "host_enqueue_ms": round(st1["enqueue_ms"], 2),
+                                       "pool_growths": st1["pool_growths"], "pinned_allocs": st1["pinned_allocs"],
+                                       "batches": st1["batches"], "mean_batch_images": round(st1["mean_batch_images"], 2),
+                                       "p50_ms": round(st1["p50_us"] / 1e3, 3), "p99_ms": round(st1["p99_us"] / 1e3, 3)},
+                        "poisson": {"rate_rps": round(rate, 1), "offered_mpix_s": round(rate * total_px / n_req / 1e6, 1),
+                                    "achieved_mpix_s": round(total_px / poisson_s / 1e6, 2),
+                                    "p50_ms": round(st2["p50_us"] / 1e3, 3), "p99_ms": round(st2["p99_us"] / 1e3, 3),
+                                    "max_ms": round(st2["max_us"] / 1e3, 3), "batches": st2["batches"],
+                                    "mean_batch_images": round(st2["mean_batch_images"], 2)}},
+            "plain_gpu_path": {"value": round(plain, 2), "unit": "Mpixel/s", "requests": n_plain,
+                               "what": "one request per launch sequence, host buffers"},
+            "speedup_vs_plain": round(value / plain, 2),
+            "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "gpu_launches": int(st1["launches"]),
+            "clocks": clk.summary()}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c4", "c1"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c4", "c1", "c5"])
+    ap.add_argument("--requests", type=int, default=0, help="c5: requests in the stream (default 2000)")
+    ap.add_argument("--rate", type=float, default=0.0, help="c5: Poisson arrival rate, requests/s")
+    ap.add_argument("--depth", type=int, default=2, help="c5: batches in flight")
+    ap.add_argument("--batch-mpix", type=float, default=128, help="c5: pixel cap of one batch (Mpixel)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="small batch for smoke runs")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
@@ -322,7 +465,10 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = tdist
     try:
-        run_gpu(args, rank, world, dist)
+        if args.workload == "c5":
+            run_serve(args, rank, world, dist)
+        else:
+            run_gpu(args, rank, world, dist)
     finally:
         if dist:
             dist.destroy_process_group()

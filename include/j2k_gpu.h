@@ -104,7 +104,8 @@ int j2k_gpu_batch_launch(j2k_gpu_ctx *ctx, void *stream);
  * sync to decode the same staged batch again. */
 int j2k_gpu_batch_stage(j2k_gpu_ctx *ctx, void *stream);
 int j2k_gpu_batch_run(j2k_gpu_ctx *ctx, void *stream);
-/* Wait for the batch with a host-side timeout (ms, < 0 = forever). */
+/* Wait for the batch with a host-side timeout (ms, < 0 = forever, 0 = poll once and return
+ * J2K_ERR_TIMEOUT while the batch is still running). */
 int j2k_gpu_batch_sync(j2k_gpu_ctx *ctx, int timeout_ms);
 /* Per-image status after sync: J2K_OK or J2K_ERR_DECODE; `bad_blocks` may be NULL. */
 int j2k_gpu_image_status(const j2k_gpu_ctx *ctx, int slot, int *bad_blocks);

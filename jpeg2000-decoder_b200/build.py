@@ -21,7 +21,7 @@ ORACLE = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_T1 = os.path.join(ROOT, "oracle", "_ref", "libref_t1.so")
 
 CU_SOURCES = ["engine.cu", "noalloc.cu"]
-CPP_SOURCES = ["codestream.cpp", "plan_api.cpp", "bmi_decoder.cpp", "bmi_jp2dec.cpp"]
+CPP_SOURCES = ["codestream.cpp", "plan_api.cpp", "bmi_decoder.cpp", "bmi_jp2dec.cpp", "server.cpp"]
 HEADERS = ["plan.h", "codestream.h", "t1_kernel.cuh", "dwt_kernel.cuh", "bmi_engine.h"]
 
 

@@ -594,10 +594,11 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   size_t o_byt = align_up(o_otk + otasks.size() * sizeof(OutTask), 256);
   size_t total = align_up(o_byt + S.bytes + 16, 256);
   if (c->h_stage_cap < total) {
+    // grow by half again at least: page-locking is slow and freeing it synchronises
+    const size_t nc = std::max(total, c->h_stage_cap * 3 / 2);
     if (c->h_stage) cudaFreeHost(c->h_stage);
     c->h_stage = nullptr;
     c->h_stage_cap = 0;
-    size_t nc = std::max(total, c->h_stage_cap * 3 / 2);
     if (cudaMallocHost(&c->h_stage, nc) != cudaSuccess) {
       cudaGetLastError();
       return J2K_ERR_NOMEM;
@@ -734,14 +735,15 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->ev[3], st));
   if (c->h_status_cap < G.n_cblks + 1) {
+    const size_t nc = std::max(G.n_cblks + 1, c->h_status_cap * 3 / 2);
     if (c->h_status) cudaFreeHost(c->h_status);
     c->h_status = nullptr;
     c->h_status_cap = 0;
-    if (cudaMallocHost(&c->h_status, (G.n_cblks + 1) * 2) != cudaSuccess) {
+    if (cudaMallocHost(&c->h_status, nc * 2) != cudaSuccess) {
       cudaGetLastError();
       return J2K_ERR_NOMEM;
     }
-    c->h_status_cap = G.n_cblks + 1;
+    c->h_status_cap = nc;
   }
   if (G.n_cblks) CK(cudaMemcpyAsync(c->h_status, c->d_status.p, G.n_cblks * 2, cudaMemcpyDeviceToHost, st));
   CK(cudaEventRecord(c->ev[4], st));
@@ -766,6 +768,7 @@ extern "C" int j2k_gpu_batch_sync(j2k_gpu_ctx *c, int timeout_ms) {
     cudaError_t e = cudaEventQuery(c->ev[4]);
     if (e == cudaSuccess) break;
     if (e != cudaErrorNotReady) return J2K_ERR_CUDA;
+    if (timeout_ms == 0) return J2K_ERR_TIMEOUT;  // poll once
     if (timeout_ms >= 0) {
       auto el = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
       if (el > timeout_ms) return J2K_ERR_TIMEOUT;

@@ -29,6 +29,7 @@ FMT_BYTES = {0: 4, 1: 6, 2: 3, 3: 4, 4: 8, 5: 6, 6: 3, 8: 8}
 FLAG_REF_COMPAT = 1
 
 J2K_OK = 0
+J2K_ERR_PARSE = -2
 J2K_ERR_NODEVICE = -9
 J2K_ERR_DECODE = -7
 J2K_ERR_TIMEOUT = -6
@@ -68,6 +69,19 @@ class Tuning(ctypes.Structure):
                 ("t1_form", ctypes.c_int), ("t1_latency_waves", ctypes.c_int)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("mem_budget", ctypes.c_size_t), ("pipeline_depth", ctypes.c_int),
+                ("max_batch_images", ctypes.c_int), ("max_batch_pixels", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("mean_batch_images", ctypes.c_double), ("p50_us", ctypes.c_double), ("p99_us", ctypes.c_double),
+                ("max_us", ctypes.c_double), ("busy_s", ctypes.c_double), ("pixels", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("gpu_ms", ctypes.c_double), ("stage_ms", ctypes.c_double),
+                ("enqueue_ms", ctypes.c_double), ("pool_growths", ctypes.c_uint64), ("pinned_allocs", ctypes.c_uint64)]
+
+
 class EncParams(ctypes.Structure):
     _fields_ = [("reversible", ctypes.c_int), ("levels", ctypes.c_int), ("cbw_exp", ctypes.c_int),
                 ("cbh_exp", ctypes.c_int), ("tile_w", ctypes.c_int), ("tile_h", ctypes.c_int),
@@ -90,6 +104,9 @@ EXPORTS = [
     "j2k_gpu_image_status", "j2k_gpu_output_device", "j2k_gpu_output_copy", "j2k_gpu_component_copy",
     "j2k_gpu_coefficients_copy", "j2k_gpu_last_timing", "j2k_gpu_last_launches", "j2k_gpu_set_tuning",
     "j2k_gpu_get_tuning", "j2k_gpu_decode", "j2k_gpu_tile_idwt_noalloc",
+    "j2k_server_create", "j2k_server_destroy", "j2k_server_submit", "j2k_server_wait", "j2k_server_result",
+    "j2k_server_latency_us",
+    "j2k_server_release", "j2k_server_drain", "j2k_server_stats_get", "j2k_server_stats_reset",
     "BMI_dec_info", "BMI_dec_init", "BMI_dec_isr", "BMI_dec", "BMI_dec_thumbnail", "BMI_dec_exit",
     "bmi_decoder_init", "bmi_decoder_set_job", "bmi_decoder_decode", "bmi_decoder_predecode",
     "bmi_decoder_status", "bmi_decoder_result", "bmi_decoder_thumbnail", "bmi_decoder_component_int",
@@ -138,6 +155,18 @@ def lib():
         L.j2k_gpu_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.j2k_gpu_decode.argtypes = [vp, ctypes.c_char_p, sz, i, i, vp, sz]
         L.j2k_gpu_tile_idwt_noalloc.argtypes = [ctypes.POINTER(TileComp), i, i, vp, vp, i, vp]
+        L.j2k_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.j2k_server_destroy.argtypes = [vp]
+        L.j2k_server_destroy.restype = None
+        L.j2k_server_submit.argtypes = [vp, ctypes.c_char_p, sz, i, i]
+        L.j2k_server_submit.restype = ctypes.c_int64
+        L.j2k_server_wait.argtypes = [vp, ctypes.c_int64, vp, sz, ctypes.POINTER(sz), i]
+        L.j2k_server_result.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(vp), ctypes.POINTER(sz), i]
+        L.j2k_server_latency_us.argtypes = [vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_double)]
+        L.j2k_server_release.argtypes = [vp, ctypes.c_int64]
+        L.j2k_server_drain.argtypes = [vp]
+        L.j2k_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.j2k_server_stats_reset.argtypes = [vp]
         L.bmi_decoder_init.argtypes = [i, i]
         L.bmi_decoder_set_job.argtypes = [i, i, ctypes.c_uint, i]
         L.bmi_decoder_set_job.restype = None
@@ -370,3 +399,80 @@ class GpuContext:
         out = self.output(slot) if fmt != FMT_NONE else None
         rc, bad = self.status(slot)
         return out, rc, bad, plan
+
+
+class Server:
+    """Continuous-batching decode service (include/j2k_server.h): submit codestreams as they
+    arrive, wait for each result; pending requests are merged into shared launches."""
+
+    def __init__(self, device=0, mem_budget=0, pipeline_depth=2, max_batch_images=0, max_batch_pixels=0):
+        cfg = ServerConfig(device, mem_budget, pipeline_depth, max_batch_images, max_batch_pixels)
+        h = ctypes.c_void_p()
+        rc = lib().j2k_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != J2K_OK:
+            raise J2kError(rc, "server_create")
+        self.h = h
+
+    def submit(self, codestream, fmt, flags=0):
+        rid = lib().j2k_server_submit(self.h, codestream, len(codestream), fmt, flags)
+        if rid < 0:
+            raise J2kError(int(rid), "server_submit")
+        return rid
+
+    def wait(self, rid, out=None, timeout_ms=-1):
+        """Returns (status, bytes); copies the output into `out` (a uint8 numpy array)."""
+        n = ctypes.c_size_t()
+        ptr = out.ctypes.data_as(ctypes.c_void_p) if out is not None else None
+        cap = out.nbytes if out is not None else 0
+        rc = lib().j2k_server_wait(self.h, rid, ptr, cap, ctypes.byref(n), timeout_ms)
+        return rc, n.value
+
+    def result(self, rid):
+        rc, n = self.wait(rid)
+        if rc != J2K_OK:
+            raise J2kError(rc, "server request %d" % rid)
+        out = np.empty(n, np.uint8)
+        rc, _ = self.wait(rid, out)
+        if rc != J2K_OK:
+            raise J2kError(rc, "server request %d" % rid)
+        return out
+
+    def view(self, rid, timeout_ms=-1):
+        """(status, zero-copy uint8 view of the output, valid until release)."""
+        ptr, n = ctypes.c_void_p(), ctypes.c_size_t()
+        rc = lib().j2k_server_result(self.h, rid, ctypes.byref(ptr), ctypes.byref(n), timeout_ms)
+        if rc != J2K_OK or not ptr.value or not n.value:
+            return rc, None
+        return rc, np.ctypeslib.as_array((ctypes.c_uint8 * n.value).from_address(ptr.value))
+
+    def latency_us(self, rid):
+        v = ctypes.c_double()
+        rc = lib().j2k_server_latency_us(self.h, rid, ctypes.byref(v))
+        if rc != J2K_OK:
+            raise J2kError(rc, "server_latency")
+        return v.value
+
+    def release(self, rid):
+        lib().j2k_server_release(self.h, rid)
+
+    def drain(self):
+        lib().j2k_server_drain(self.h)
+
+    def stats(self):
+        st = ServerStats()
+        lib().j2k_server_stats_get(self.h, ctypes.byref(st))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        lib().j2k_server_stats_reset(self.h)
+
+    def close(self):
+        if self.h:
+            lib().j2k_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

@@ -146,6 +146,18 @@ def c5_request(seed):
     return cs, h * w
 
 
+def c5_format(cs):
+    """Packed RGB output format of a serving request: 24-bit for 8-bit pictures, 48-bit above."""
+    plan = native.Plan(cs)
+    return native.FMT_24BITS_RGB if plan.info.bitdepth <= 8 else native.FMT_48BITS_RGB
+
+
+def c5_pool(n_distinct=48, seed=5, workers=None):
+    """Distinct serving requests (codestreams) from per-request seeds."""
+    with ThreadPoolExecutor(max_workers=workers or 4) as ex:
+        return [cs for cs, _ in ex.map(c5_request, [seed * 100000 + i for i in range(n_distinct)])]
+
+
 # ------------------------------------------------------------------ workloads ---------
 def _cached(key, make):
     os.makedirs(CACHE, exist_ok=True)
@@ -189,4 +201,11 @@ def workload(name, quick=False):
         cfg = {"workload": "C1 512x512 gray 5/3 lossless", "frames": 1, "size": "512x512", "components": 1,
                "bitdepth": 8, "wavelet": "5/3", "levels": 5, "codeblock": "64x64", "layers": 1}
         return cfg, streams, native.FMT_32BITS_4COMPONENTS
+    if name == "c5":
+        nd = 12 if quick else 48
+        streams = _cached("c5-v1-%d" % nd, lambda: c5_pool(nd, workers=os.cpu_count()))
+        cfg = {"workload": "C5 serving stream", "distinct_requests": nd,
+               "sizes": ["256x256", "512x512", "1024x1024", "1920x1080", "4096x2160"],
+               "mix": "half 8-bit 5/3+RCT lossless, half 8/12-bit 9/7+ICT at 0.5-2 bpp", "codeblock": "64x64"}
+        return cfg, streams, None
     raise SystemExit("unknown workload " + name)

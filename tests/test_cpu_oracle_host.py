@@ -195,3 +195,6 @@ def test_no_cpu_fallback_without_device(pkg):
     assert e.value.code == native.J2K_ERR_NODEVICE
     # the reference-facing C API reports failure instead of decoding on the CPU
     assert native.lib().bmi_decoder_init(1, 1) != 0
+    with pytest.raises(native.J2kError) as e:
+        native.Server()
+    assert e.value.code == native.J2K_ERR_NODEVICE
