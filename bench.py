@@ -187,6 +187,10 @@ def run_gpu(args, rank, world, dist):
     for p in plans:
         ctx.add(p, fmt)
     ctx.stage(sp)
+    tuned = None
+    if not args.no_autotune:
+        tuned, _ = ctx.autotune(2, sp)
+    ctx.set_tuning(use_graph=0 if args.no_graph else 1)
     for _ in range(args.warmup):
         ctx.run(sp)
         assert ctx.sync() == 0
@@ -220,6 +224,7 @@ def run_gpu(args, rank, world, dist):
         total_ms = float(t.item())
     value = pixels * world * args.steps / (total_ms / 1e3) / 1e6
 
+    ctx.set_tuning(use_graph=0)  # the batches below are decoded once each: nothing to replay
     # ---- plain per-image GPU path: one image per launch sequence
     plain_ms = []
     uniq = plans[: min(len(plans), 16)]
@@ -278,7 +283,9 @@ def run_gpu(args, rank, world, dist):
     clocks = clk.summary()
     cfg = dict(cfg)
     cfg.update({"parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",
-                "bad_blocks": bad})
+                "bad_blocks": bad, "cuda_graph": not args.no_graph,
+                "autotuned_t1": ({"form": "compact" if tuned["t1_form"] == 1 else "unrolled",
+                                  "warps_per_cta": tuned["t1_warps_per_cta"]} if tuned else None)})
     line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (9/7) / int32 (5/3)", "data": "synthetic (seeded, project encoder)",
@@ -449,6 +456,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="small batch for smoke runs")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-autotune", action="store_true", help="skip the Tier-1 shape autotuner")
+    ap.add_argument("--no-graph", action="store_true", help="enqueue launches instead of replaying a CUDA graph")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -22,6 +22,7 @@
 #include <cstring>
 #include <new>
 #include <thread>
+#include <map>
 #include <vector>
 
 #include "../../include/j2k_gpu.h"
@@ -222,11 +223,25 @@ struct j2k_gpu_ctx {
   float t_t1 = 0, t_dwt = 0, t_h2d = 0, t_total = 0;
   int launches = 0;
   j2k_gpu_tuning tuning{8, 64, 0, 0, 2};
+  cudaGraphExec_t gexec = nullptr;  // captured decode of the staged batch (tuning.use_graph)
+  int graph_launches = 0;
+  // autotuned Tier-1 shape per queue-length bucket (floor(log2(code-blocks))): kernel form
+  // (1 compact, 2 unrolled) and warps per CTA; consulted by the auto form
+  struct TuneEntry {
+    int form = 0, warps = 0;
+    float t1_ms = 0;
+  };
+  std::map<int, TuneEntry> tune_table;
   int sm_count = 148;
   size_t smem_optin = 227 * 1024;
 };
 
 namespace {
+
+void drop_graph(j2k_gpu_ctx *c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+}
 
 int cuda_fail(cudaError_t e) {
   (void)e;
@@ -312,6 +327,7 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
 
 extern "C" void j2k_gpu_ctx_destroy(j2k_gpu_ctx *c) {
   if (!c) return;
+  drop_graph(c);
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf *all[] = {&c->d_bytes, &c->d_cblks, &c->d_order, &c->d_seg,    &c->d_status, &c->d_counter,
@@ -340,8 +356,12 @@ extern "C" int j2k_gpu_set_tuning(j2k_gpu_ctx *c, const j2k_gpu_tuning *t) {
   if (n.t1_warps_per_cta <= 0) n.t1_warps_per_cta = 8;
   if (n.t1_warps_per_cta > 32) n.t1_warps_per_cta = 32;
   if (n.dwt_tile <= 0) n.dwt_tile = 64;
+  if (n.dwt_tile != 64) return J2K_ERR_UNSUPPORTED;  // the level kernels are built for 64x64 tiles
   if (n.t1_form < 0 || n.t1_form > 2) n.t1_form = 0;
   if (n.t1_latency_waves <= 0) n.t1_latency_waves = 2;
+  if (n.use_graph != c->tuning.use_graph || n.t1_form != c->tuning.t1_form ||
+      n.t1_warps_per_cta != c->tuning.t1_warps_per_cta || n.t1_latency_waves != c->tuning.t1_latency_waves)
+    drop_graph(c);
   c->tuning = n;
   return J2K_OK;
 }
@@ -413,11 +433,11 @@ namespace {
 // shared memory and thread limits from the occupancy calculator), one wave of CTAs.
 template <int MAXW, int MAXH, bool UNROLLED>
 void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
-                  const uint32_t *seg, const T1Tables *tab) {
+                  const uint32_t *seg, const T1Tables *tab, int warps_per_cta) {
   typedef T1Layout<MAXW, MAXH> Lay;
   const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
   int best_w = 1, best_ctas = 1, best_warps = 0;
-  const int wmax = c->tuning.t1_warps_per_cta > 0 ? std::min(8, c->tuning.t1_warps_per_cta) : 8;
+  const int wmax = warps_per_cta > 0 ? std::min(8, warps_per_cta) : 8;
   for (int w = 1; w <= wmax; ++w) {
     const size_t sm = tsz + (size_t)w * Lay::PER_WARP;
     if (sm > c->smem_optin) break;
@@ -446,16 +466,23 @@ template <int MAXW, int MAXH>
 void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
                const uint32_t *seg, const T1Tables *tab) {
   bool unrolled;
+  int warps = c->tuning.t1_warps_per_cta;
   if (c->tuning.t1_form == 1) {
     unrolled = false;
   } else if (c->tuning.t1_form == 2) {
     unrolled = true;
   } else {
-    const int waves = c->tuning.t1_latency_waves > 0 ? c->tuning.t1_latency_waves : 2;
-    unrolled = (long long)n <= (long long)waves * c->sm_count * 32;
+    auto it = c->tune_table.find(n > 0 ? 31 - __builtin_clz((unsigned)n) : 0);
+    if (it != c->tune_table.end()) {
+      unrolled = it->second.form == 2;
+      warps = it->second.warps;
+    } else {
+      const int waves = c->tuning.t1_latency_waves > 0 ? c->tuning.t1_latency_waves : 2;
+      unrolled = (long long)n <= (long long)waves * c->sm_count * 32;
+    }
   }
-  if (unrolled) launch_t1_as<MAXW, MAXH, true>(c, st, n, cbs, ord, cnt, seg, tab);
-  else launch_t1_as<MAXW, MAXH, false>(c, st, n, cbs, ord, cnt, seg, tab);
+  if (unrolled) launch_t1_as<MAXW, MAXH, true>(c, st, n, cbs, ord, cnt, seg, tab, warps);
+  else launch_t1_as<MAXW, MAXH, false>(c, st, n, cbs, ord, cnt, seg, tab, warps);
 }
 }  // namespace
 
@@ -657,18 +684,34 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   c->sg.o_otk = o_otk;
   c->sg.maxL = maxL;
   c->sg.dtask_off = dtask_off;
+  if (c->h_status_cap < S.cblks + 1) {
+    const size_t nc = std::max(S.cblks + 1, c->h_status_cap * 3 / 2);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    c->h_status = nullptr;
+    c->h_status_cap = 0;
+    if (cudaMallocHost(&c->h_status, nc * 2) != cudaSuccess) {
+      cudaGetLastError();
+      return J2K_ERR_NOMEM;
+    }
+    c->h_status_cap = nc;
+  }
+  drop_graph(c);  // a captured decode belongs to the previous batch
   c->staged = true;
   c->launched = false;
   c->synced = false;
   return J2K_OK;
 }
 
-extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
-  if (!c) return J2K_ERR_ARG;
-  if (!c->staged || (c->launched && !c->synced)) return J2K_ERR_STATE;
-  cudaSetDevice(c->device);
-  cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
-  c->user_stream = st;
+namespace {
+// Event record that also fires when captured into a graph and replayed
+cudaError_t record(cudaEvent_t ev, cudaStream_t st, bool capturing) {
+  return capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
+}
+
+// Everything one decode of the staged batch enqueues after its input copies: counter reset,
+// the Tier-1 launch, the DWT level launches, the output stage, the status read-back and the
+// bracketing events.
+int enqueue_decode(j2k_gpu_ctx *c, cudaStream_t st, bool capturing) {
   const auto &G = c->sg;
   uint8_t *D = (uint8_t *)c->d_cblks.p;
   const size_t o_cbs = G.o_cbs, o_ord = G.o_ord, o_seg = G.o_seg, o_lev = G.o_lev, o_dtk = G.o_dtk, o_grp = G.o_grp,
@@ -681,12 +724,6 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
     bool empty() const { return n == 0; }
   } otasks{G.n_otasks};
   c->launches = 0;
-  if (!c->launched) {
-    // first run after staging: the staging events already bracket the copies
-  } else {
-    CK(cudaEventRecord(c->ev[0], st));
-    CK(cudaEventRecord(c->ev[1], st));
-  }
   CK(cudaMemsetAsync(c->d_counter.p, 0, 64, st));
 
   // ---- Tier-1
@@ -705,7 +742,7 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
     qoff += G.nq[q];
   }
   CK(cudaGetLastError());
-  CK(cudaEventRecord(c->ev[2], st));
+  CK(record(c->ev[2], st, capturing));
 
   // ---- inverse DWT, coarsest level step first
   const DwtLevel *d_lev = (const DwtLevel *)(D + o_lev);
@@ -733,20 +770,59 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
     c->launches++;
   }
   CK(cudaGetLastError());
-  CK(cudaEventRecord(c->ev[3], st));
-  if (c->h_status_cap < G.n_cblks + 1) {
-    const size_t nc = std::max(G.n_cblks + 1, c->h_status_cap * 3 / 2);
-    if (c->h_status) cudaFreeHost(c->h_status);
-    c->h_status = nullptr;
-    c->h_status_cap = 0;
-    if (cudaMallocHost(&c->h_status, nc * 2) != cudaSuccess) {
-      cudaGetLastError();
-      return J2K_ERR_NOMEM;
-    }
-    c->h_status_cap = nc;
-  }
+  CK(record(c->ev[3], st, capturing));
   if (G.n_cblks) CK(cudaMemcpyAsync(c->h_status, c->d_status.p, G.n_cblks * 2, cudaMemcpyDeviceToHost, st));
-  CK(cudaEventRecord(c->ev[4], st));
+  CK(record(c->ev[4], st, capturing));
+  return J2K_OK;
+}
+
+// Capture the decode of the staged batch into a graph (once per staged batch).  Returns
+// false when capture is unavailable, in which case the caller enqueues the launches
+// directly; either way the same kernels run.
+bool capture_decode(j2k_gpu_ctx *c, cudaStream_t st) {
+  if (c->gexec) return true;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const int rc = enqueue_decode(c, st, true);
+  const cudaError_t e = cudaStreamEndCapture(st, &g);
+  if (rc != J2K_OK || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return false;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&c->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    c->gexec = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  c->graph_launches = c->launches;
+  return true;
+}
+}  // namespace
+
+extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
+  if (!c) return J2K_ERR_ARG;
+  if (!c->staged || (c->launched && !c->synced)) return J2K_ERR_STATE;
+  cudaSetDevice(c->device);
+  cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
+  c->user_stream = st;
+  if (c->launched) {
+    // a repeated run: no input copies, both copy events at the start
+    CK(cudaEventRecord(c->ev[0], st));
+    CK(cudaEventRecord(c->ev[1], st));
+  }  // else the first run after staging: the staging events already bracket the copies
+  if (c->tuning.use_graph && capture_decode(c, st)) {
+    CK(cudaGraphLaunch(c->gexec, st));
+    c->launches = c->graph_launches;
+  } else {
+    const int rc = enqueue_decode(c, st, false);
+    if (rc != J2K_OK) return rc;
+  }
   c->launched = true;
   c->synced = false;
   return J2K_OK;
@@ -873,6 +949,50 @@ extern "C" int j2k_gpu_last_timing(const j2k_gpu_ctx *c, float *t1, float *dwt, 
   if (dwt) *dwt = c->t_dwt;
   if (h2d) *h2d = c->t_h2d;
   if (total) *total = c->t_total;
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_autotune(j2k_gpu_ctx *c, void *stream, int iters, j2k_gpu_tuning *best, float *best_ms) {
+  if (!c || iters <= 0) return J2K_ERR_ARG;
+  if (!c->staged || (c->launched && !c->synced)) return J2K_ERR_STATE;
+  const j2k_gpu_tuning saved = c->tuning;
+  const int n = (int)c->sg.nq[Q64];
+  const int bucket = n > 0 ? 31 - __builtin_clz((unsigned)n) : 0;
+  j2k_gpu_ctx::TuneEntry win;
+  win.t1_ms = 1e30f;
+  static const int forms[2] = {1, 2};
+  static const int widths[3] = {2, 4, 8};
+  for (int f : forms)
+    for (int w : widths) {
+      j2k_gpu_tuning t = saved;
+      t.t1_form = f;
+      t.t1_warps_per_cta = w;
+      t.use_graph = 0;
+      int rc = j2k_gpu_set_tuning(c, &t);
+      float tmin = 1e30f;
+      for (int i = 0; rc == J2K_OK && i <= iters; ++i) {
+        if ((rc = j2k_gpu_batch_run(c, stream)) != J2K_OK || (rc = j2k_gpu_batch_sync(c, -1)) != J2K_OK) break;
+        if (i > 0) tmin = std::min(tmin, c->t_t1);  // the first run warms caches and clocks
+      }
+      if (rc != J2K_OK) {
+        c->tuning = saved;
+        return rc;
+      }
+      if (tmin < win.t1_ms) {
+        win.t1_ms = tmin;
+        win.form = f;
+        win.warps = w;
+      }
+    }
+  c->tune_table[bucket] = win;
+  c->tuning = saved;
+  drop_graph(c);
+  if (best) {
+    *best = saved;
+    best->t1_form = win.form;
+    best->t1_warps_per_cta = win.warps;
+  }
+  if (best_ms) *best_ms = win.t1_ms;
   return J2K_OK;
 }
 

@@ -103,7 +103,7 @@ EXPORTS = [
     "j2k_gpu_batch_add", "j2k_gpu_batch_footprint", "j2k_gpu_batch_launch", "j2k_gpu_batch_stage", "j2k_gpu_batch_run", "j2k_gpu_batch_sync",
     "j2k_gpu_image_status", "j2k_gpu_output_device", "j2k_gpu_output_copy", "j2k_gpu_component_copy",
     "j2k_gpu_coefficients_copy", "j2k_gpu_last_timing", "j2k_gpu_last_launches", "j2k_gpu_set_tuning",
-    "j2k_gpu_get_tuning", "j2k_gpu_decode", "j2k_gpu_tile_idwt_noalloc",
+    "j2k_gpu_get_tuning", "j2k_gpu_autotune", "j2k_gpu_decode", "j2k_gpu_tile_idwt_noalloc",
     "j2k_server_create", "j2k_server_destroy", "j2k_server_submit", "j2k_server_wait", "j2k_server_result",
     "j2k_server_latency_us",
     "j2k_server_release", "j2k_server_drain", "j2k_server_stats_get", "j2k_server_stats_reset",
@@ -153,6 +153,7 @@ def lib():
         L.j2k_gpu_last_launches.argtypes = [vp, ctypes.POINTER(i)]
         L.j2k_gpu_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.j2k_gpu_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.j2k_gpu_autotune.argtypes = [vp, vp, i, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float)]
         L.j2k_gpu_decode.argtypes = [vp, ctypes.c_char_p, sz, i, i, vp, sz]
         L.j2k_gpu_tile_idwt_noalloc.argtypes = [ctypes.POINTER(TileComp), i, i, vp, vp, i, vp]
         L.j2k_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
@@ -383,6 +384,18 @@ class GpuContext:
     def set_tuning(self, t1_warps_per_cta=0, dwt_tile=0, use_graph=0, t1_form=0, t1_latency_waves=0):
         t = Tuning(t1_warps_per_cta, dwt_tile, use_graph, t1_form, t1_latency_waves)
         self._ck(lib().j2k_gpu_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
+
+    def get_tuning(self):
+        t = Tuning()
+        self._ck(lib().j2k_gpu_get_tuning(self.h, ctypes.byref(t)), "get_tuning")
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+
+    def autotune(self, iters=2, stream=None):
+        """Time the staged batch under each Tier-1 form / CTA width; the auto form then uses
+        the winner for batches of this size.  Returns (winner tuning dict, Tier-1 ms)."""
+        t, ms = Tuning(), ctypes.c_float()
+        self._ck(lib().j2k_gpu_autotune(self.h, stream, iters, ctypes.byref(t), ctypes.byref(ms)), "autotune")
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}, ms.value
 
     def mem_usage(self):
         r, b = ctypes.c_size_t(), ctypes.c_size_t()

@@ -256,3 +256,36 @@ def test_corrupt_blocks_do_not_hang(gpu_ctx):
         assert gpu_ctx.sync(timeout_ms=20000) == 0
         orc, oout, _ = oracle_util.oracle_decode(plan, native.FMT_24BITS_RGB)
         assert np.array_equal(gpu_ctx.output(0), oout)
+
+
+def test_autotune_and_graph_replay_match_direct_launches(gpu_ctx):
+    """The autotuner's trial runs and a replayed CUDA graph of the staged batch give the
+    same pictures as direct launches (tolerance 0), and the graph is re-captured after the
+    batch changes."""
+    from jpeg2000_decoder_b200 import native, synth
+    frames = synth.video_frames(3, n=2)
+    streams = [native.encode(f, 8, **synth.C3_PARAMS) for f in frames]
+    plans = [native.Plan(cs) for cs in streams]
+    want = [gpu_ctx.decode(cs, native.FMT_24BITS_RGB)[0].copy() for cs in streams]
+    gpu_ctx.begin()
+    for p in plans:
+        gpu_ctx.add(p, native.FMT_24BITS_RGB)
+    gpu_ctx.stage()
+    best, ms = gpu_ctx.autotune(1)
+    assert best["t1_form"] in (1, 2) and best["t1_warps_per_cta"] in (2, 4, 8) and ms > 0
+    gpu_ctx.set_tuning(use_graph=1)
+    for _ in range(2):
+        gpu_ctx.run()
+        assert gpu_ctx.sync() == 0
+        for i in range(len(plans)):
+            assert np.array_equal(gpu_ctx.output(i), want[i])
+    assert gpu_ctx.launches() >= 3
+    # a new batch (one picture) replaces the captured graph
+    gpu_ctx.begin()
+    gpu_ctx.add(plans[1], native.FMT_24BITS_RGB)
+    gpu_ctx.launch()
+    assert gpu_ctx.sync() == 0
+    assert np.array_equal(gpu_ctx.output(0), want[1])
+    gpu_ctx.set_tuning()
+    with pytest.raises(native.J2kError):
+        gpu_ctx.set_tuning(dwt_tile=32)  # only 64x64 DWT tiles are built
