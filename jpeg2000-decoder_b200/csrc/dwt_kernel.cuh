@@ -5,7 +5,8 @@
  * One CTA reconstructs a 64x64 output tile of one resolution level of one
  * tile-component: it stages the 72x72 interleaved input window (the four quadrants of the
  * Mallat layout plus a 4-sample whole-sample-symmetric halo) in shared memory with
- * coalesced loads, runs the horizontal then the vertical lifting steps there, and writes
+ * coalesced asynchronous copies, lifts each window row and then each output column in
+ * registers (one thread streams one line), and writes
  * the 64x64 result with coalesced stores.  Every level is one read and one write of the
  * level's samples; all tile-components of a batch at a given level share one launch.
  *
@@ -179,21 +180,30 @@ __device__ __forceinline__ void dwt_tile(DwtSmem<REV> &S, const typename DwtType
     else S.srow[w] = src;
   }
   __syncthreads();
-  // stage quadrant by quadrant: consecutive threads read consecutive source columns
+  // stage quadrant by quadrant with asynchronous 4-byte copies (cp.async): every thread
+  // issues all of its loads before waiting, so a CTA has its whole window in flight;
+  // consecutive threads read consecutive source columns
   constexpr int QN = DWT_N / 2;  // 36 window lines of each parity
+  const uint32_t tile_s = (uint32_t)__cvta_generic_to_shared(tile);
   for (int e = threadIdx.x; e < 4 * QN * QN; e += blockDim.x) {
     const int qd = e / (QN * QN), r = (e - qd * QN * QN) / QN, j = e - qd * QN * QN - r * QN;
     const int iy = 2 * r + (qd >> 1), ix = 2 * j + (qd & 1);
-    T v;
-    if (qd == 0) {
-      v = llsrc[(size_t)S.srow[iy] * stride_ll + S.scol[ix]];
-      if (!REV && ll_gain) v = (T)__fmul_rn((float)v, gain);
-    } else {
-      v = quad[(size_t)S.srow[iy] * stride_q + S.scol[ix]];
-    }
-    tile[iy * DWT_PITCH + ix] = v;
+    const T *src = qd == 0 ? llsrc + (size_t)S.srow[iy] * stride_ll + S.scol[ix]
+                           : quad + (size_t)S.srow[iy] * stride_q + S.scol[ix];
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tile_s + 4u * (iy * DWT_PITCH + ix)), "l"(src)
+                 : "memory");
   }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
+  if (!REV && ll_gain) {
+    // the reconstructed LL entering a finer 9/7 level is scaled by K_lo^2
+    for (int e = threadIdx.x; e < QN * QN; e += blockDim.x) {
+      const int r = e / QN, j = e - r * QN;
+      T *v = tile + 2 * r * DWT_PITCH + 2 * j;
+      *v = (T)__fmul_rn((float)*v, gain);
+    }
+    __syncthreads();
+  }
   if (rw > 1) {
     for (int r = threadIdx.x; r < DWT_N; r += blockDim.x) lift_line<REV>(tile + r * DWT_PITCH, 1);
     __syncthreads();
