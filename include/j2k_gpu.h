@@ -56,8 +56,13 @@ enum {
 
 /* decode flags */
 enum {
-  J2K_FLAG_REF_COMPAT = 0x1 /* reproduce the reference's 5/3 column-end arithmetic
-                               (bmi_cpu_dwt_decoder.cpp:3364-3398) instead of T.800 */
+  J2K_FLAG_REF_COMPAT = 0x1, /* reproduce the reference's 5/3 column-end arithmetic
+                                (bmi_cpu_dwt_decoder.cpp:3364-3398) instead of T.800 */
+  J2K_FLAG_KEEP_COMPONENTS = 0x2 /* keep the reconstructed components in device memory for
+                                    j2k_gpu_component_copy / coefficients_copy(stage 1).
+                                    Without it an image with a packed output format has its
+                                    last DWT level fused with the inverse MCT and pack, which
+                                    never stores the components. */
 };
 
 /* ---------------------------------------------------------------- host plans (Tier-2) */
@@ -114,7 +119,8 @@ int j2k_gpu_output_device(const j2k_gpu_ctx *ctx, int slot, const void **dptr, s
 int j2k_gpu_output_copy(j2k_gpu_ctx *ctx, int slot, void *host_dst, size_t bytes);
 /* Decoded (un-shifted) component samples of a slot as int32 (5/3) or float32 (9/7),
  * row-major over the output size: the reference's GetDecodedComponentInt / Float
- * (decoder/core/src/decoderconcrete.cpp:531-584). */
+ * (decoder/core/src/decoderconcrete.cpp:531-584).  J2K_ERR_STATE for an image added with a
+ * packed format and without J2K_FLAG_KEEP_COMPONENTS. */
 int j2k_gpu_component_copy(j2k_gpu_ctx *ctx, int slot, int comp, void *host_dst, size_t bytes);
 /* Parity hooks: the coefficient buffer of a slot after Tier-1 (stage 0) or after the
  * inverse DWT of every tile-component (stage 1), in the plan's Mallat layout. */

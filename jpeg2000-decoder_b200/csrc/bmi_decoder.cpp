@@ -326,8 +326,9 @@ class GpuDecoder : public Decoder {
     if (s.pending) finish_pending();
     if (s.status != READY || comp < 0 || comp >= s.props.mComponentNum) return false;
     if (s.comp_loaded == comp) return true;
-    if (resident_ != s.handler) {
-      // device buffers hold another picture: decode this one again (components only)
+    // decode the picture again with its components kept (when the device buffers hold
+    // another picture, or this picture's packed decode fused its last level with the output)
+    auto redecode = [&]() {
       finish_pending();
       j2k_plan *p = nullptr;
       if (j2k_plan_create(s.codestream.data(), s.codestream.size(), discard_of_slot(s), 0, s.cfg.mIgnoreComponents,
@@ -338,15 +339,24 @@ class GpuDecoder : public Decoder {
           j2k_gpu_batch_launch(ctx_, nullptr) != J2K_OK || j2k_gpu_batch_sync(ctx_, -1) != J2K_OK)
         return false;
       resident_ = s.handler;
-    }
+      return true;
+    };
+    if (resident_ != s.handler && !redecode()) return false;
     const size_t n = (size_t)s.props.mOutputSize.x * s.props.mOutputSize.y;
+    void *dst;
     if (s.props.mMethod == Ckernels_W5X3) {
       s.comp_int.resize(n);
-      if (j2k_gpu_component_copy(ctx_, s.gpu_slot, comp, s.comp_int.data(), n * 4) != J2K_OK) return false;
+      dst = s.comp_int.data();
     } else {
       s.comp_float.resize(n);
-      if (j2k_gpu_component_copy(ctx_, s.gpu_slot, comp, s.comp_float.data(), n * 4) != J2K_OK) return false;
+      dst = s.comp_float.data();
     }
+    int rc = j2k_gpu_component_copy(ctx_, s.gpu_slot, comp, dst, n * 4);
+    if (rc == J2K_ERR_STATE) {
+      if (!redecode()) return false;
+      rc = j2k_gpu_component_copy(ctx_, s.gpu_slot, comp, dst, n * 4);
+    }
+    if (rc != J2K_OK) return false;
     s.comp_loaded = comp;
     return true;
   }

@@ -24,6 +24,7 @@
  */
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 namespace j2k_dev {
 
@@ -89,7 +90,8 @@ struct DwtTypes<false> {
   typedef float T;
 };
 
-constexpr int DWT_THREADS = 128;  // threads per CTA of the level kernels
+constexpr int DWT_THREADS = 128;    // threads per CTA of the level kernels
+constexpr int FUSED_THREADS = 256;  // threads per CTA of the fused last-level + output kernel
 
 // Lifting of one window line (72 samples, element stride `st`), streamed by one thread
 // through registers: iteration m reads the pair (x[2m], x[2m+1]) and retires the samples
@@ -157,62 +159,76 @@ struct DwtSmem {
   int32_t srow[DWT_N], scol[DWT_N];
 };
 
-// One 64x64 output tile of one level.  `quad`: the level's Mallat quadrants (LL taken from
-// `llsrc` instead, scaled by `gain` when ll_gain); output to `out`.
+// Inputs of one window: the level's Mallat quadrants (`quad`) and the LL quadrant
+// (`llsrc`, another buffer for every level but the first)
 template <bool REV>
-__device__ __forceinline__ void dwt_tile(DwtSmem<REV> &S, const typename DwtTypes<REV>::T *quad, int stride_q,
-                                         const typename DwtTypes<REV>::T *llsrc, int stride_ll,
-                                         typename DwtTypes<REV>::T *out, int stride_out, int rw, int rh, int lw,
-                                         int lh, bool ll_gain, float gain, bool refcompat, int ox, int oy) {
+struct WinSrc {
+  const typename DwtTypes<REV>::T *quad;
+  int stride_q;
+  const typename DwtTypes<REV>::T *llsrc;
+  int stride_ll;
+};
+
+// Rebuild the 64x64 output tile at (ox, oy) of one level for `nw` windows of the same
+// geometry (the components of one tile at their last level, or one tile-component): the
+// results are left in the centre of each window, S[w].tile[(y + 4) * DWT_PITCH + x + 4].
+template <bool REV>
+__device__ __forceinline__ void dwt_windows(DwtSmem<REV> *S, int nw, const WinSrc<REV> *src, int rw, int rh, int lw,
+                                            int lh, bool ll_gain, float gain, bool refcompat, int ox, int oy) {
   typedef typename DwtTypes<REV>::T T;
-  T *tile = S.tile;
   // source line of every window row / column: window index i <-> position o - 4 + i, whose
   // mirror keeps its parity, so even window lines come from the low part and odd ones
-  // from the high part
+  // from the high part (the same for every window)
   for (int i = threadIdx.x; i < 2 * DWT_N; i += blockDim.x) {
     const bool col = i >= DWT_N;
     const int w = col ? i - DWT_N : i;
     const int n = col ? rw : rh, lo = col ? lw : lh;
     // the window may reach far past a level smaller than the tile: full periodic mirror
     const int x = mirror((col ? ox : oy) - DWT_H + w, n);
-    const int src = (x & 1) ? lo + (x >> 1) : (x >> 1);
-    if (col) S.scol[w] = src;
-    else S.srow[w] = src;
+    const int sl = (x & 1) ? lo + (x >> 1) : (x >> 1);
+    if (col) S[0].scol[w] = sl;
+    else S[0].srow[w] = sl;
   }
   __syncthreads();
   // stage quadrant by quadrant with asynchronous 4-byte copies (cp.async): every thread
-  // issues all of its loads before waiting, so a CTA has its whole window in flight;
+  // issues all of its loads before waiting, so a CTA has all its windows in flight;
   // consecutive threads read consecutive source columns
   constexpr int QN = DWT_N / 2;  // 36 window lines of each parity
-  const uint32_t tile_s = (uint32_t)__cvta_generic_to_shared(tile);
-  for (int e = threadIdx.x; e < 4 * QN * QN; e += blockDim.x) {
-    const int qd = e / (QN * QN), r = (e - qd * QN * QN) / QN, j = e - qd * QN * QN - r * QN;
-    const int iy = 2 * r + (qd >> 1), ix = 2 * j + (qd & 1);
-    const T *src = qd == 0 ? llsrc + (size_t)S.srow[iy] * stride_ll + S.scol[ix]
-                           : quad + (size_t)S.srow[iy] * stride_q + S.scol[ix];
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tile_s + 4u * (iy * DWT_PITCH + ix)), "l"(src)
-                 : "memory");
+  for (int w = 0; w < nw; ++w) {
+    const uint32_t tile_s = (uint32_t)__cvta_generic_to_shared(S[w].tile);
+    const WinSrc<REV> in = src[w];
+    for (int e = threadIdx.x; e < 4 * QN * QN; e += blockDim.x) {
+      const int qd = e / (QN * QN), r = (e - qd * QN * QN) / QN, j = e - qd * QN * QN - r * QN;
+      const int iy = 2 * r + (qd >> 1), ix = 2 * j + (qd & 1);
+      const T *p = qd == 0 ? in.llsrc + (size_t)S[0].srow[iy] * in.stride_ll + S[0].scol[ix]
+                           : in.quad + (size_t)S[0].srow[iy] * in.stride_q + S[0].scol[ix];
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tile_s + 4u * (iy * DWT_PITCH + ix)), "l"(p)
+                   : "memory");
+    }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   if (!REV && ll_gain) {
     // the reconstructed LL entering a finer 9/7 level is scaled by K_lo^2
-    for (int e = threadIdx.x; e < QN * QN; e += blockDim.x) {
-      const int r = e / QN, j = e - r * QN;
-      T *v = tile + 2 * r * DWT_PITCH + 2 * j;
+    for (int e = threadIdx.x; e < nw * QN * QN; e += blockDim.x) {
+      const int w = e / (QN * QN), q = e - w * QN * QN, r = q / QN, j = q - r * QN;
+      T *v = S[w].tile + 2 * r * DWT_PITCH + 2 * j;
       *v = (T)__fmul_rn((float)*v, gain);
     }
     __syncthreads();
   }
   if (rw > 1) {
-    for (int r = threadIdx.x; r < DWT_N; r += blockDim.x) lift_line<REV>(tile + r * DWT_PITCH, 1);
+    for (int l = threadIdx.x; l < nw * DWT_N; l += blockDim.x) {
+      const int w = l / DWT_N, r = l - w * DWT_N;
+      lift_line<REV>(S[w].tile + r * DWT_PITCH, 1);
+    }
     __syncthreads();
   }
   // reference-compat: keep the horizontally transformed inputs the column end reads
   const int n = rh;
   const bool fix = REV && refcompat && n >= 3 && (oy <= n - 1) && (n - 2 < oy + DWT_T);
+  int rowA = -1, rowB = -1;
   if (fix) {
-    int rowA, rowB = -1;
     if (!(n & 1)) {
       rowA = n - 3;  // H[m-2]
     } else {
@@ -220,26 +236,31 @@ __device__ __forceinline__ void dwt_tile(DwtSmem<REV> &S, const typename DwtType
       rowA = n - 3;                 // L[m-2]
       rowB = (m >= 3) ? n - 4 : 1;  // H[m-3] (H[0] when m == 2)
     }
-    for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
-      S.keep[0][c] = tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
-      if (rowB >= 0) S.keep[1][c] = tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+    for (int e = threadIdx.x; e < nw * DWT_T; e += blockDim.x) {
+      const int w = e / DWT_T, c = e - w * DWT_T;
+      S[w].keep[0][c] = S[w].tile[(rowA - oy + DWT_H) * DWT_PITCH + DWT_H + c];
+      if (rowB >= 0) S[w].keep[1][c] = S[w].tile[(rowB - oy + DWT_H) * DWT_PITCH + DWT_H + c];
     }
     __syncthreads();
   }
   if (rh > 1) {
-    for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) lift_line<REV>(tile + DWT_H + c, DWT_PITCH);
+    for (int l = threadIdx.x; l < nw * DWT_T; l += blockDim.x) {
+      const int w = l / DWT_T, c = l - w * DWT_T;
+      lift_line<REV>(S[w].tile + DWT_H + c, DWT_PITCH);
+    }
     __syncthreads();
   }
   if constexpr (REV) {
     if (fix) {
-      for (int c = threadIdx.x; c < DWT_T; c += blockDim.x) {
-        T *col = tile + DWT_H + c;
+      for (int e = threadIdx.x; e < nw * DWT_T; e += blockDim.x) {
+        const int w = e / DWT_T, c = e - w * DWT_T;
+        T *col = S[w].tile + DWT_H + c;
         const int r1 = n - 1 - oy + DWT_H, r2 = n - 2 - oy + DWT_H, r3 = n - 3 - oy + DWT_H;
         if (!(n & 1)) {
-          col[r1 * DWT_PITCH] = S.keep[0][c] + col[r2 * DWT_PITCH];
+          col[r1 * DWT_PITCH] = S[w].keep[0][c] + col[r2 * DWT_PITCH];
         } else {
-          const T hx = S.keep[1][c];
-          const T x1 = S.keep[0][c] - ((hx + 1) >> 1);
+          const T hx = S[w].keep[1][c];
+          const T x1 = S[w].keep[0][c] - ((hx + 1) >> 1);
           col[r1 * DWT_PITCH] = x1;
           col[r2 * DWT_PITCH] = hx + ((x1 + col[r3 * DWT_PITCH]) >> 1);
         }
@@ -247,11 +268,21 @@ __device__ __forceinline__ void dwt_tile(DwtSmem<REV> &S, const typename DwtType
       __syncthreads();
     }
   }
-  // write the 64x64 result
+}
+
+// One 64x64 output tile of one level of one tile-component, stored to `out`.
+template <bool REV>
+__device__ __forceinline__ void dwt_tile(DwtSmem<REV> &S, const typename DwtTypes<REV>::T *quad, int stride_q,
+                                         const typename DwtTypes<REV>::T *llsrc, int stride_ll,
+                                         typename DwtTypes<REV>::T *out, int stride_out, int rw, int rh, int lw,
+                                         int lh, bool ll_gain, float gain, bool refcompat, int ox, int oy) {
+  const WinSrc<REV> src{quad, stride_q, llsrc, stride_ll};
+  dwt_windows<REV>(&S, 1, &src, rw, rh, lw, lh, ll_gain, gain, refcompat, ox, oy);
   const int ow = min(DWT_T, rw - ox), oh = min(DWT_T, rh - oy);
   for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
     const int yy = i / DWT_T, xx = i % DWT_T;
-    if (yy < oh && xx < ow) out[(size_t)(oy + yy) * stride_out + ox + xx] = tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
+    if (yy < oh && xx < ow)
+      out[(size_t)(oy + yy) * stride_out + ox + xx] = S.tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
   }
   __syncthreads();
 }
@@ -300,84 +331,147 @@ __device__ __forceinline__ void put_slot(uint8_t *px, int pxb, int slot, int v) 
   else ((uint16_t *)px)[3 - slot] = (uint16_t)v;
 }
 
+// Last level of every component of one tile with the output stage fused into its store:
+// the components' windows stay in shared memory and the packed pixels are the only write.
+struct FusedGroup {
+  OutGroup G;
+  uint64_t base[3];  // element offset of each component's region (same in every buffer)
+  int8_t ll_src[3];  // buffer of each component's LL quadrant: 0 coefficients, 1 B, 2 C
+  int8_t ll_gain, refcompat;
+  int32_t stride, rw, rh, lw, lh;
+};
+
+// Inverse RCT / ICT + DC level shift + clamp + LIFT + pack of one pixel (bmi_cpu_dwt_decoder.cpp
+// RICT_97_FLOAT :3570-3643, RRct_53 :3936-4130, MergeComponents :4283-4598).  `v[c]` is
+// component c's reconstructed sample (int32 for 5/3, float for 9/7), `have[c]` whether the
+// component is present.
+template <typename T>
+__device__ __forceinline__ void emit_pixel(const OutGroup &G, uint8_t *out, int yy, int xx, const T *v,
+                                           const bool *have) {
+  constexpr bool INT = std::is_integral<T>::value;
+  const int pxb = fmt_bytes(G.fmt);
+  const int B = G.bitdepth;
+  const int outdepth = (pxb == 3 || pxb == 4) ? 8 : 16;
+  const int maxv = (1 << B) - 1, dc = 1 << (B - 1);
+  const bool rgb = (G.fmt == 0 || G.fmt == 1 || G.fmt == 2 || G.fmt == 8);
+  const bool do_mct = rgb && G.mct && G.ncomp >= 3 && have[1] && have[2];
+  const int slot0 = (pxb == 4 || pxb == 8) ? 1 : 0;
+  uint8_t *px = out + G.out_off + ((size_t)(G.y0 + yy) * G.pitch_px + (G.x0 + xx)) * pxb;
+  uint8_t tmp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (do_mct) {
+    int c3[3];
+    if constexpr (INT) {
+      const int y = v[0], u = v[1], w = v[2];
+      const int g = y - ((u + w) >> 2) + dc;
+      c3[0] = clampi(w + g, maxv);
+      c3[1] = clampi(g, maxv);
+      c3[2] = clampi(u + g, maxv);
+    } else {
+      const float y = v[0], u = v[1], w = v[2];
+      const float sh = (float)dc, fm = (float)maxv;
+      float t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.402f, w)), sh);
+      c3[0] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+      t = __fadd_rn(__fadd_rn(__fadd_rn(y, __fmul_rn(-0.34413f, u)), __fmul_rn(-0.71414f, w)), sh);
+      c3[1] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+      t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.772f, u)), sh);
+      c3[2] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+    }
+    if (G.checkout >= 0 && G.checkout < 3) {
+      // one component replicated into R, G and B (RICT_97_FLOAT / RRct_53 case 0..2)
+      const int vv = lift_depth(c3[G.checkout], B, outdepth);
+      for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k + slot0, vv);
+    } else {
+      for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k + slot0, lift_depth(c3[k], B, outdepth));
+    }
+  } else if (G.checkout >= 0 && have[G.checkout]) {
+    // MergeComponents with a checked-out component: value in R = G = B, and in the
+    // alpha slot only for the 4-component formats (bmi_cpu_dwt_decoder.cpp:4300-4308)
+    const int vv = lift_depth(clampi((int)v[G.checkout] + dc, maxv), B, outdepth);
+    if (pxb == 3 || pxb == 6) {
+      for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k, vv);
+    } else {
+      for (int k = 1; k < 4; ++k) put_slot(tmp, pxb, k, vv);
+      if (G.fmt == 3 || G.fmt == 4) put_slot(tmp, pxb, 0, vv);
+    }
+  } else {
+    for (int c = 0; c < G.ncomp && c < 4; ++c) {
+      if (!have[c]) continue;
+      if ((pxb == 3 || pxb == 6) && c > 2) continue;
+      put_slot(tmp, pxb, c, lift_depth(clampi((int)v[c] + dc, maxv), B, outdepth));
+    }
+  }
+  for (int k = 0; k < pxb; ++k) px[k] = tmp[k];
+}
+
 #ifndef J2K_DWT_LEVELS_ONLY
-// Inverse RCT / ICT + DC level shift + clamp + LIFT + pack (bmi_cpu_dwt_decoder.cpp
-// RICT_97_FLOAT :3570-3643, RRct_53 :3936-4130, MergeComponents :4283-4598).
+// Output stage for tiles whose last level was not fused: reads the reconstructed
+// components from the level buffers.
 __global__ void __launch_bounds__(256) output_kernel(const OutGroup *__restrict__ groups,
                                                      const OutTask *__restrict__ tasks, int ntasks, const void *bufA,
                                                      const void *bufB, const void *bufC, uint8_t *out) {
   for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
     const OutTask tk = tasks[task];
     const OutGroup G = groups[tk.group];
-    const int pxb = fmt_bytes(G.fmt);
-    const int B = G.bitdepth;
-    const int outdepth = (pxb == 3 || pxb == 4) ? 8 : 16;
-    const int maxv = (1 << B) - 1, dc = 1 << (B - 1);
-    const bool rgb = (G.fmt == 0 || G.fmt == 1 || G.fmt == 2 || G.fmt == 8);
-    const bool do_mct = rgb && G.mct && G.ncomp >= 3 && G.comp_buf[1] >= 0 && G.comp_buf[2] >= 0;
-    const int slot0 = (pxb == 4 || pxb == 8) ? 1 : 0;
     const void *cb[4];
+    bool have[4];
     for (int c = 0; c < 4; ++c) {
       const void *bb = G.comp_buf[c] == 0 ? bufA : (G.comp_buf[c] == 1 ? bufB : bufC);
       cb[c] = G.comp_buf[c] < 0 ? nullptr : (const void *)((const uint8_t *)bb + G.comp_off[c] * 4);
+      have[c] = cb[c] != nullptr;
     }
     const int ox = tk.tx * 64, oy = tk.ty * 64;
     for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
       const int yy = oy + i / 64, xx = ox + i % 64;
       if (yy >= G.h || xx >= G.w) continue;
-      uint8_t *px = out + G.out_off + ((size_t)(G.y0 + yy) * G.pitch_px + (G.x0 + xx)) * pxb;
-      uint8_t tmp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (do_mct) {
-        const size_t o0 = (size_t)yy * G.stride[0] + xx, o1 = (size_t)yy * G.stride[1] + xx,
-                     o2 = (size_t)yy * G.stride[2] + xx;
-        int v[3];
-        if (G.rev) {
-          const int y = ((const int32_t *)cb[0])[o0], u = ((const int32_t *)cb[1])[o1], w = ((const int32_t *)cb[2])[o2];
-          const int g = y - ((u + w) >> 2) + dc;
-          v[0] = clampi(w + g, maxv);
-          v[1] = clampi(g, maxv);
-          v[2] = clampi(u + g, maxv);
-        } else {
-          const float y = ((const float *)cb[0])[o0], u = ((const float *)cb[1])[o1], w = ((const float *)cb[2])[o2];
-          const float sh = (float)dc, fm = (float)maxv;
-          float t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.402f, w)), sh);
-          v[0] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
-          t = __fadd_rn(__fadd_rn(__fadd_rn(y, __fmul_rn(-0.34413f, u)), __fmul_rn(-0.71414f, w)), sh);
-          v[1] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
-          t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.772f, u)), sh);
-          v[2] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
-        }
-        if (G.checkout >= 0 && G.checkout < 3) {
-          // one component replicated into R, G and B (RICT_97_FLOAT / RRct_53 case 0..2)
-          const int vv = lift_depth(v[G.checkout], B, outdepth);
-          for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k + slot0, vv);
-        } else {
-          for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k + slot0, lift_depth(v[k], B, outdepth));
-        }
-      } else if (G.checkout >= 0 && cb[G.checkout]) {
-        // MergeComponents with a checked-out component: value in R = G = B, and in the
-        // alpha slot only for the 4-component formats (bmi_cpu_dwt_decoder.cpp:4300-4308)
-        const size_t o = (size_t)yy * G.stride[G.checkout] + xx;
-        int v = G.rev ? ((const int32_t *)cb[G.checkout])[o] : (int)((const float *)cb[G.checkout])[o];
-        v = lift_depth(clampi(v + dc, maxv), B, outdepth);
-        if (pxb == 3 || pxb == 6) {
-          for (int k = 0; k < 3; ++k) put_slot(tmp, pxb, k, v);
-        } else {
-          for (int k = 1; k < 4; ++k) put_slot(tmp, pxb, k, v);
-          if (G.fmt == 3 || G.fmt == 4) put_slot(tmp, pxb, 0, v);
-        }
+      if (G.rev) {
+        int32_t v[4] = {0, 0, 0, 0};
+        for (int c = 0; c < 4; ++c)
+          if (have[c]) v[c] = ((const int32_t *)cb[c])[(size_t)yy * G.stride[c] + xx];
+        emit_pixel<int32_t>(G, out, yy, xx, v, have);
       } else {
-        for (int c = 0; c < G.ncomp && c < 4; ++c) {
-          if (!cb[c]) continue;
-          if ((pxb == 3 || pxb == 6) && c > 2) continue;
-          const size_t o = (size_t)yy * G.stride[c] + xx;
-          int v = G.rev ? ((const int32_t *)cb[c])[o] : (int)((const float *)cb[c])[o];
-          v = clampi(v + dc, maxv);
-          put_slot(tmp, pxb, c, lift_depth(v, B, outdepth));
-        }
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int c = 0; c < 4; ++c)
+          if (have[c]) v[c] = ((const float *)cb[c])[(size_t)yy * G.stride[c] + xx];
+        emit_pixel<float>(G, out, yy, xx, v, have);
       }
-      for (int k = 0; k < pxb; ++k) px[k] = tmp[k];
     }
+  }
+}
+
+// Last DWT level of up to three components of one tile fused with the output stage (the
+// inverse MCT reads the components' windows in shared memory): one CTA per 64x64 tile.
+// Dynamic shared memory: `nwin` DwtSmem windows.
+template <bool REV>
+__global__ void __launch_bounds__(FUSED_THREADS) last_level_output_kernel(const FusedGroup *__restrict__ groups,
+                                                                        const OutTask *__restrict__ tasks, int ntasks,
+                                                                        void *bufA, void *bufB, void *bufC,
+                                                                        float ll_gain_value, uint8_t *out) {
+  typedef typename DwtTypes<REV>::T T;
+  extern __shared__ __align__(16) uint8_t dsm[];
+  DwtSmem<REV> *S = reinterpret_cast<DwtSmem<REV> *>(dsm);
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const OutTask tk = tasks[task];
+    const FusedGroup &F = groups[tk.group];
+    const OutGroup G = F.G;
+    const int nc = min(3, (int)G.ncomp);
+    WinSrc<REV> src[3];
+    bool have[4] = {false, false, false, false};
+    for (int c = 0; c < nc; ++c) {
+      const T *A = dwt_buf<REV>(0, bufA, bufB, bufC) + F.base[c];
+      src[c] = {A, F.stride, dwt_buf<REV>(F.ll_src[c], bufA, bufB, bufC) + F.base[c], F.stride};
+      have[c] = true;
+    }
+    const int ox = tk.tx * DWT_T, oy = tk.ty * DWT_T;
+    dwt_windows<REV>(S, nc, src, F.rw, F.rh, F.lw, F.lh, F.ll_gain != 0, ll_gain_value, F.refcompat != 0, ox, oy);
+    const int ow = min(DWT_T, F.rw - ox), oh = min(DWT_T, F.rh - oy);
+    for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
+      const int yy = i / DWT_T, xx = i % DWT_T;
+      if (yy >= oh || xx >= ow) continue;
+      T v[4] = {0, 0, 0, 0};
+      for (int c = 0; c < nc; ++c) v[c] = S[c].tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
+      emit_pixel<T>(G, out, oy + yy, ox + xx, v, have);
+    }
+    __syncthreads();
   }
 }
 #endif  // J2K_DWT_LEVELS_ONLY

@@ -196,6 +196,7 @@ struct BatchImage {
   uint64_t coef_base, out_base, out_bytes;
   uint32_t cblk_base;
   int status, bad;
+  bool fused;  // last DWT level fused with the output stage: components not kept
 };
 
 }  // namespace
@@ -215,7 +216,9 @@ struct j2k_gpu_ctx {
   // staged batch (device-resident inputs) for batch_run
   struct Staged {
     size_t nq[NQ] = {0}, n_cblks = 0, n_otasks = 0;
-    size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0;
+    size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0, o_fgr = 0, o_ftk = 0;
+    size_t n_ftasks[2] = {0, 0};
+    int fwin = 1;
     int maxL = 0;
     std::vector<uint32_t> dtask_off;
   } sg;
@@ -321,6 +324,10 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
   // opt into the large dynamic shared memory of the Tier-1 kernels
   cudaFuncSetAttribute(t1_kernel<64, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   cudaFuncSetAttribute(t1_kernel<64, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(last_level_output_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(3 * sizeof(DwtSmem<true>)));
+  cudaFuncSetAttribute(last_level_output_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(3 * sizeof(DwtSmem<false>)));
   *out = c;
   return J2K_OK;
 }
@@ -505,6 +512,9 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::vector<std::vector<DwtTask>> steps_rev, steps_irr;
   std::vector<OutGroup> groups;
   std::vector<OutTask> otasks;
+  std::vector<FusedGroup> fgroups;
+  std::vector<OutTask> ftasks[2];  // fused last levels: [0] 9/7, [1] 5/3
+  int fwin = 1;
   uint64_t byte_base = 0;
   uint32_t seg_base = 0;
   int maxL = 0;
@@ -528,6 +538,28 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
     seg_base += (uint32_t)p.seglens.size();
     const bool rev = p.info.reversible != 0;
     const int refc = (im.flags & J2K_FLAG_REF_COMPAT) ? 1 : 0;
+    // Tiles whose last level is fused with the output stage: packed output wanted, no
+    // component kept for the getters, 1-3 components of one size, all with >= 1 level
+    std::vector<char> fuse(p.tilecomps.size(), 0);
+    im.fused = false;
+    if (im.fmt != J2K_FMT_NONE && im.checkout < 0 && !(im.flags & J2K_FLAG_KEEP_COMPONENTS)) {
+      for (size_t t = 0; t < p.tilecomps.size(); ++t) {
+        const j2k_tilecomp &tc = p.tilecomps[t];
+        if (tc.comp != 0) continue;
+        bool ok = tc.levels >= 1;
+        int nc = 0;
+        for (size_t u = 0; u < p.tilecomps.size() && ok; ++u) {
+          const j2k_tilecomp &tu = p.tilecomps[u];
+          if (tu.tile != tc.tile) continue;
+          nc++;
+          ok = tu.comp < 3 && tu.levels == tc.levels && tu.w == tc.w && tu.h == tc.h;
+        }
+        if (!ok || nc < 1 || nc > 3) continue;
+        for (size_t u = 0; u < p.tilecomps.size(); ++u)
+          if (p.tilecomps[u].tile == tc.tile) fuse[u] = 1;
+        im.fused = true;
+      }
+    }
     // DWT levels of every tile-component, aligned so that all finish at the last step
     std::vector<int8_t> final_buf(p.tilecomps.size());
     for (size_t t = 0; t < p.tilecomps.size(); ++t) {
@@ -547,6 +579,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
         L.ll_gain = (!rev && r > 1) ? 1 : 0;
         L.refcompat = (int8_t)refc;
         if (L.rw <= 0 || L.rh <= 0) continue;
+        if (r == Lt && fuse[t]) continue;  // rebuilt by the fused output stage
         L.tiles_x = (L.rw + DWT_T - 1) / DWT_T;
         const int tiles_y = (L.rh + DWT_T - 1) / DWT_T;
         const uint32_t li = (uint32_t)levels.size();
@@ -562,6 +595,48 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       for (size_t t = 0; t < p.tilecomps.size(); ++t) {
         const j2k_tilecomp &tc = p.tilecomps[t];
         if (tc.comp != 0) continue;
+        if (fuse[t]) {
+          FusedGroup F{};
+          OutGroup &G = F.G;
+          for (int k = 0; k < 4; ++k) G.comp_buf[k] = -1;
+          int nc = 0;
+          const int Lt = tc.levels;
+          for (size_t u = 0; u < p.tilecomps.size(); ++u) {
+            const j2k_tilecomp &tu = p.tilecomps[u];
+            if (tu.tile != tc.tile) continue;
+            F.base[tu.comp] = im.coef_base + tu.coef_off;
+            F.ll_src[tu.comp] = Lt == 1 ? 0 : (((Lt - 1) & 1) ? 1 : 2);
+            G.comp_buf[tu.comp] = 0;
+            G.stride[tu.comp] = tu.w;
+            nc = std::max(nc, tu.comp + 1);
+          }
+          F.ll_gain = (!rev && Lt > 1) ? 1 : 0;
+          F.refcompat = (int8_t)refc;
+          F.stride = tc.w;
+          F.rw = tc.res_w[Lt];
+          F.rh = tc.res_h[Lt];
+          F.lw = tc.res_w[Lt - 1];
+          F.lh = tc.res_h[Lt - 1];
+          G.x0 = tc.x0;
+          G.y0 = tc.y0;
+          G.w = tc.w;
+          G.h = tc.h;
+          G.out_off = im.out_base;
+          G.pitch_px = p.info.width;
+          G.fmt = (int16_t)im.fmt;
+          G.bitdepth = (int16_t)p.info.bitdepth;
+          G.rev = (int8_t)rev;
+          G.mct = (int8_t)p.info.mct;
+          G.ncomp = (int8_t)nc;
+          G.checkout = -1;
+          G.tiles_x = (tc.w + DWT_T - 1) / DWT_T;
+          fwin = std::max(fwin, nc);
+          const uint32_t gi = (uint32_t)fgroups.size();
+          fgroups.push_back(F);
+          for (int ty = 0; ty < (tc.h + DWT_T - 1) / DWT_T; ++ty)
+            for (int tx = 0; tx < G.tiles_x; ++tx) ftasks[rev ? 1 : 0].push_back({gi, (uint16_t)tx, (uint16_t)ty});
+          continue;
+        }
         OutGroup G{};
         for (int k = 0; k < 4; ++k) G.comp_buf[k] = -1;
         int nc = 0;
@@ -618,7 +693,9 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   size_t o_dtk = align_up(o_lev + levels.size() * sizeof(DwtLevel), 256);
   size_t o_grp = align_up(o_dtk + dtasks.size() * sizeof(DwtTask), 256);
   size_t o_otk = align_up(o_grp + groups.size() * sizeof(OutGroup), 256);
-  size_t o_byt = align_up(o_otk + otasks.size() * sizeof(OutTask), 256);
+  size_t o_fgr = align_up(o_otk + otasks.size() * sizeof(OutTask), 256);
+  size_t o_ftk = align_up(o_fgr + fgroups.size() * sizeof(FusedGroup), 256);
+  size_t o_byt = align_up(o_ftk + (ftasks[0].size() + ftasks[1].size()) * sizeof(OutTask), 256);
   size_t total = align_up(o_byt + S.bytes + 16, 256);
   if (c->h_stage_cap < total) {
     // grow by half again at least: page-locking is slow and freeing it synchronises
@@ -646,6 +723,9 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::memcpy(H + o_dtk, dtasks.data(), dtasks.size() * sizeof(DwtTask));
   std::memcpy(H + o_grp, groups.data(), groups.size() * sizeof(OutGroup));
   std::memcpy(H + o_otk, otasks.data(), otasks.size() * sizeof(OutTask));
+  std::memcpy(H + o_fgr, fgroups.data(), fgroups.size() * sizeof(FusedGroup));
+  std::memcpy(H + o_ftk, ftasks[0].data(), ftasks[0].size() * sizeof(OutTask));
+  std::memcpy(H + o_ftk + ftasks[0].size() * sizeof(OutTask), ftasks[1].data(), ftasks[1].size() * sizeof(OutTask));
   {
     size_t off = o_byt;
     for (auto &im : c->imgs) {
@@ -675,6 +755,11 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   for (int q = 0; q < NQ; ++q) c->sg.nq[q] = ordq[q].size();
   c->sg.n_cblks = S.cblks;
   c->sg.n_otasks = otasks.size();
+  c->sg.o_fgr = o_fgr;
+  c->sg.o_ftk = o_ftk;
+  c->sg.n_ftasks[0] = ftasks[0].size();
+  c->sg.n_ftasks[1] = ftasks[1].size();
+  c->sg.fwin = fwin;
   c->sg.o_cbs = o_cbs;
   c->sg.o_ord = o_ord;
   c->sg.o_seg = o_seg;
@@ -762,6 +847,20 @@ int enqueue_decode(j2k_gpu_ctx *c, cudaStream_t st, bool capturing) {
                                                                          c->d_A.p, c->d_B.p, c->d_C.p, llg);
       c->launches++;
     }
+  }
+  for (int k = 0; k < 2; ++k) {
+    const int nf = (int)G.n_ftasks[k];
+    if (!nf) continue;
+    const OutTask *ft = (const OutTask *)(D + G.o_ftk) + (k ? G.n_ftasks[0] : 0);
+    const FusedGroup *fg = (const FusedGroup *)(D + G.o_fgr);
+    if (k) {
+      last_level_output_kernel<true><<<std::min(nf, dwt_cap), FUSED_THREADS, G.fwin * sizeof(DwtSmem<true>), st>>>(
+          fg, ft, nf, c->d_A.p, c->d_B.p, c->d_C.p, llg, (uint8_t *)c->d_out.p);
+    } else {
+      last_level_output_kernel<false><<<std::min(nf, dwt_cap), FUSED_THREADS, G.fwin * sizeof(DwtSmem<false>), st>>>(
+          fg, ft, nf, c->d_A.p, c->d_B.p, c->d_C.p, llg, (uint8_t *)c->d_out.p);
+    }
+    c->launches++;
   }
   if (!otasks.empty()) {
     output_kernel<<<std::min((int)otasks.size(), dwt_cap), 256, 0, st>>>(
@@ -908,6 +1007,7 @@ extern "C" int j2k_gpu_coefficients_copy(j2k_gpu_ctx *c, int slot, int stage, vo
   const BatchImage &im = c->imgs[slot];
   const auto &p = im.plan->p;
   if (bytes < p.info.coef_elems * 4) return J2K_ERR_ARG;
+  if (stage == 1 && im.fused) return J2K_ERR_STATE;  // last level fused with the output stage
   cudaSetDevice(c->device);
   for (const j2k_tilecomp &tc : p.tilecomps) {
     const int Lt = tc.levels;
@@ -927,6 +1027,7 @@ extern "C" int j2k_gpu_component_copy(j2k_gpu_ctx *c, int slot, int comp, void *
   const auto &p = im.plan->p;
   const size_t need = (size_t)p.info.width * p.info.height * 4;
   if (bytes < need || comp < 0 || comp >= p.info.ncomp) return J2K_ERR_ARG;
+  if (im.fused) return J2K_ERR_STATE;  // last level fused with the output stage
   cudaSetDevice(c->device);
   bool found = false;
   for (const j2k_tilecomp &tc : p.tilecomps) {

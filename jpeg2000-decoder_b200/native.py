@@ -27,6 +27,7 @@ FMT_64BITS_ARGB = 8
 FMT_BYTES = {0: 4, 1: 6, 2: 3, 3: 4, 4: 8, 5: 6, 6: 3, 8: 8}
 
 FLAG_REF_COMPAT = 1
+FLAG_KEEP_COMPONENTS = 2
 
 J2K_OK = 0
 J2K_ERR_PARSE = -2

@@ -289,3 +289,28 @@ def test_autotune_and_graph_replay_match_direct_launches(gpu_ctx):
     gpu_ctx.set_tuning()
     with pytest.raises(native.J2kError):
         gpu_ctx.set_tuning(dwt_tile=32)  # only 64x64 DWT tiles are built
+
+
+@pytest.mark.parametrize("name", ["rgb300x200_97_tiles_3layers.j2k", "rgb12_53_bypass_reset.j2k", "c1_gray_53.j2k"])
+def test_fused_last_level_equals_kept_components_path(gpu_ctx, name):
+    """A packed output normally comes from the last DWT level fused with the inverse MCT and
+    pack; J2K_FLAG_KEEP_COMPONENTS takes the separate level + output kernels instead.  Both
+    give the same picture (tolerance 0), and only the latter keeps the components."""
+    from jpeg2000_decoder_b200 import native
+    cs = _read(name)
+    plan = native.Plan(cs)
+    fmt = native.FMT_32BITS_4COMPONENTS if plan.info.ncomp == 1 else (
+        native.FMT_48BITS_RGB if plan.info.bitdepth > 8 else native.FMT_24BITS_RGB)
+    outs = []
+    for flags in (0, native.FLAG_KEEP_COMPONENTS):
+        gpu_ctx.begin()
+        gpu_ctx.add(plan, fmt, flags)
+        gpu_ctx.launch()
+        assert gpu_ctx.sync() == 0
+        outs.append(gpu_ctx.output(0).copy())
+        if flags:
+            assert gpu_ctx.component(0, 0).size == plan.info.width * plan.info.height
+        else:
+            with pytest.raises(native.J2kError):
+                gpu_ctx.component(0, 0)
+    assert np.array_equal(outs[0], outs[1])
