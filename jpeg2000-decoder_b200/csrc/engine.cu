@@ -62,10 +62,10 @@ struct T1Layout {
 enum { Q64 = 0, NQ = 1 };
 
 template <int MAXW, int MAXH, bool UNROLLED>
-__global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order,
-                                                 int n, int *__restrict__ counter, const uint8_t *__restrict__ bytes,
-                                                 const uint32_t *__restrict__ seglens, void *__restrict__ coef,
-                                                 uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab) {
+__device__ __forceinline__ void t1_body(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n,
+                                        int *__restrict__ counter, const uint8_t *__restrict__ bytes,
+                                        const uint32_t *__restrict__ seglens, void *__restrict__ coef,
+                                        uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab) {
   extern __shared__ __align__(16) uint8_t smem[];
   typedef T1Layout<MAXW, MAXH> Lay;
   T1Tables &T = *reinterpret_cast<T1Tables *>(smem);
@@ -118,6 +118,29 @@ __global__ void __launch_bounds__(256) t1_kernel(const j2k_cblk *__restrict__ cb
     if (lane == 0) status[ci] = (uint16_t)st;
     __syncwarp();
   }
+}
+
+// The two kernel forms.  The compact form keeps the default register target, which leaves
+// room for 32 resident warps per SM; the unrolled form (batches that fit one wave) may use
+// more registers, as occupancy does not bound it.
+#define J2K_T1_PARAMS                                                                                   \
+  const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n, int *__restrict__ counter, \
+      const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens, void *__restrict__ coef,   \
+      uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab
+template <int MAXW, int MAXH>
+__global__ void __launch_bounds__(256) t1_kernel_compact(J2K_T1_PARAMS) {
+  t1_body<MAXW, MAXH, false>(cbs, order, n, counter, bytes, seglens, coef, status, gtab);
+}
+template <int MAXW, int MAXH>
+__global__ void __launch_bounds__(256, 1) t1_kernel_unrolled(J2K_T1_PARAMS) {
+  t1_body<MAXW, MAXH, true>(cbs, order, n, counter, bytes, seglens, coef, status, gtab);
+}
+#undef J2K_T1_PARAMS
+
+template <int MAXW, int MAXH, bool UNROLLED>
+constexpr auto t1_kernel() {
+  if constexpr (UNROLLED) return &t1_kernel_unrolled<MAXW, MAXH>;
+  else return &t1_kernel_compact<MAXW, MAXH>;
 }
 
 // ------------------------------------------------------------------ host tables --------
@@ -322,8 +345,8 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
     return J2K_ERR_CUDA;
   }
   // opt into the large dynamic shared memory of the Tier-1 kernels
-  cudaFuncSetAttribute(t1_kernel<64, 64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
-  cudaFuncSetAttribute(t1_kernel<64, 64, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
+  cudaFuncSetAttribute(t1_kernel<64, 64, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   cudaFuncSetAttribute(last_level_output_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(3 * sizeof(DwtSmem<true>)));
   cudaFuncSetAttribute(last_level_output_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -449,7 +472,7 @@ void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, c
     const size_t sm = tsz + (size_t)w * Lay::PER_WARP;
     if (sm > c->smem_optin) break;
     int ctas = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH, UNROLLED>, w * 32, sm) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH, UNROLLED>(), w * 32, sm) !=
         cudaSuccess) {
       cudaGetLastError();
       continue;
@@ -462,7 +485,7 @@ void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, c
   }
   const size_t sm = tsz + (size_t)best_w * Lay::PER_WARP;
   const int grid = std::max(1, std::min((n + best_w - 1) / best_w, c->sm_count * std::max(1, best_ctas)));
-  t1_kernel<MAXW, MAXH, UNROLLED><<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
+  t1_kernel<MAXW, MAXH, UNROLLED>()<<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
                                                                      c->d_A.p, (uint16_t *)c->d_status.p, tab);
 }
 

@@ -335,8 +335,9 @@ constexpr uint32_t V_SIG = 0x10u, V_CHI = 1u << CHI_POS, V_MU = 1u << MU_POS, V_
 // not yet significant with a significant neighbour; a row that becomes significant can
 // make the rows below it eligible
 template <bool UNROLLED>
-__device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int col, int p,
-                                               bool israw, const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
+__device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, uint32_t todo, int row,
+                                               int col, int p, bool israw, const uint8_t *zc, Raw &raw, Mq &mq,
+                                               const T1Tables &T) {
   bool newsig = false;
   if constexpr (UNROLLED) {
 #pragma unroll
@@ -351,7 +352,6 @@ __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp,
       }
     }
   } else {
-    uint32_t todo = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw);
     while (todo) {
       const int k = __ffs(todo) - 1;
       todo &= todo - 1;
@@ -370,10 +370,9 @@ __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp,
 // magnitude refinement of one stripe column (bmi_block_decoder.cpp:217-349): rows
 // significant before this bit-plane
 template <bool UNROLLED>
-__device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, uint8_t *rf, int row, int col, int p,
-                                              bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
+__device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, uint32_t rows, uint8_t *rf, int row,
+                                              int col, int p, bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
   const uint32_t refined = *rf;
-  const uint32_t rows = row_mask<0u, V_SIG | V_MU, 0u>(cw);
 #pragma unroll
   for (int i = 0; i < (UNROLLED ? 4 : 1); ++i) {
     uint32_t todo = UNROLLED ? (rows & (1u << i)) : rows;
@@ -394,10 +393,10 @@ __device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, u
 // of the first significant sample, whose sign follows directly); then every row not yet
 // coded in this bit-plane
 template <bool UNROLLED>
-__device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int col, int p,
-                                               const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
+__device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, uint32_t todo, int row,
+                                               int col, int p, const uint8_t *zc, Raw &raw, Mq &mq,
+                                               const T1Tables &T) {
   int forced = -1;
-  uint32_t todo;
   if (cw == 0) {
     // run-length symbol, then the two uniform symbols (the reference's fixed-Qe
     // MQ_DECODE_START is an ordinary decision on a context pinned at state 46)
@@ -410,8 +409,6 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
     }
     forced = r & 3;
     todo = (0xFu << forced) & 0xFu;
-  } else {
-    todo = row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw);
   }
   bool newsig = false;
 #pragma unroll
@@ -425,8 +422,6 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
       newsig = true;
     }
   }
-  cw |= (cw << (MU_POS - 4)) & MU_ALL;
-  cw &= ~PI_ALL;
   return newsig;
 }
 
@@ -446,12 +441,31 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
     uint8_t *rrow = b.rf + s * b.gap;
     for (int c0 = 0; c0 < b.w; c0 += 32) {
       __syncwarp();
+      // lane-parallel view of the chunk (unrolled form): each lane's word and the rows its
+      // pass would visit.  While decoding, a column's word changes only when its left
+      // neighbour gains a significant sample (`dirty`); the serial loop reloads those and
+      // uses the lanes' copies for the rest.  The compact form keeps fewer values live across
+      // the serial loop (registers bound its occupancy): it reloads every word and visits
+      // every column in cleanup.
+      constexpr bool LP = UNROLLED;
       const int c = c0 + lane;
       const bool valid = c < b.w;
       const uint32_t word = valid ? row[c] : 0u;
-      const bool work = pass == P_SIGPROP ? word != 0 : (pass == P_MAGREF ? (word & MU_ALL) != 0 : true);
+      uint32_t mask = 0;
+      bool work;
+      if (pass == P_SIGPROP) {
+        if (LP) mask = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(word);
+        work = LP ? mask != 0 : word != 0;
+      } else if (pass == P_MAGREF) {
+        if (LP) mask = row_mask<0u, V_SIG | V_MU, 0u>(word);
+        work = LP ? mask != 0 : (word & MU_ALL) != 0;
+      } else {
+        if (LP) mask = row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(word);
+        work = LP ? (word == 0 || mask != 0) : true;  // run mode, or rows not yet coded
+      }
       uint32_t live = __ballot_sync(0xffffffffu, valid && work);
       uint32_t zero = __ballot_sync(0xffffffffu, valid && word == 0);
+      uint32_t dirty = 0;
       while (live) {
         const int bit = __ffs(live) - 1;
         if (pass == P_CLEANUP && ((zero >> bit) & 1)) {
@@ -471,17 +485,52 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
         live &= live - 1;
         const int col = c0 + bit;
         uint32_t *wp = row + col;
-        uint32_t cw = *wp;
+        uint32_t cw, lane_word = 0, lane_mask = 0;
+        bool dty = true;
+        if (LP) {
+          lane_word = __shfl_sync(0xffffffffu, word, bit);
+          lane_mask = __shfl_sync(0xffffffffu, mask, bit);
+          dty = (dirty >> bit) & 1;
+          cw = dty ? *wp : lane_word;
+        } else {
+          cw = *wp;
+        }
         if (pass == P_MAGREF) {
-          magref_column<UNROLLED>(b, cw, rrow + col, 4 * s, col, p, israw, raw, mq, T);
+          const uint32_t rows = LP ? lane_mask : row_mask<0u, V_SIG | V_MU, 0u>(cw);
+          magref_column<UNROLLED>(b, cw, rows, rrow + col, 4 * s, col, p, israw, raw, mq, T);
           continue;
         }
-        const bool newsig = pass == P_SIGPROP ? sigprop_column<UNROLLED>(b, wp, cw, 4 * s, col, p, israw, zc, raw, mq, T)
-                                              : cleanup_column<UNROLLED>(b, wp, cw, 4 * s, col, p, zc, raw, mq, T);
+        bool newsig;
+        if (pass == P_SIGPROP) {
+          const uint32_t todo = dty ? row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw) : lane_mask;
+          newsig = sigprop_column<UNROLLED>(b, wp, cw, todo, 4 * s, col, p, israw, zc, raw, mq, T);
+        } else {
+          // own-row bits do not change from the left, so the lane's mask holds; a column
+          // that was all-zero may have been reached from the left and is not any more
+          const uint32_t todo =
+              (dty && (!LP || lane_word == 0)) ? row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw) : lane_mask;
+          newsig = cleanup_column<UNROLLED>(b, wp, cw, todo, 4 * s, col, p, zc, raw, mq, T);
+          if (!LP) {
+            cw |= (cw << (MU_POS - 4)) & MU_ALL;  // mu |= sigma, pi cleared
+            cw &= ~PI_ALL;
+          }
+        }
         *wp = cw;
         if (newsig && bit < 31) {
           if (pass == P_SIGPROP) live |= 1u << (bit + 1);
           zero &= ~(1u << (bit + 1));
+          if (LP) dirty |= 1u << (bit + 1);
+        }
+      }
+      if (LP && pass == P_CLEANUP) {
+        // end of the bit-plane for this chunk's columns: mu |= sigma, pi cleared
+        // (bmi_block_decoder.cpp:571-573); no later decision of this pass reads a column's
+        // own mu / pi bits
+        __syncwarp();
+        if (valid) {
+          uint32_t w = row[c];
+          w |= (w << (MU_POS - 4)) & MU_ALL;
+          row[c] = w & ~PI_ALL;
         }
       }
     }
