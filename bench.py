@@ -118,6 +118,23 @@ def profile_traffic():
         return {}
 
 
+# ------------------------------------------------------------------ replicas ----------
+def max_over_ranks(seconds_or_ms, dist, device="cuda"):
+    """The slowest rank's time (the job's time): replicas decode independent copies and
+    meet only here, so the job finishes when the last one does."""
+    if not dist:
+        return float(seconds_or_ms)
+    import torch
+    t = torch.tensor([float(seconds_or_ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, world, steps, total_time_s):
+    """Whole-job units per second: every rank processed `units_per_rank` per step."""
+    return units_per_rank * world * steps / total_time_s
+
+
 # ------------------------------------------------------------------ CPU (oracle) -------
 def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
     """Decode a bounded sample of the workload with the CPU restatement on all host cores."""
@@ -218,11 +235,8 @@ def run_gpu(args, rank, world, dist):
     torch.cuda.synchronize()
     step_ms = float(np.mean(times))
     total_ms = float(np.sum(times))
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = pixels * world * args.steps / (total_ms / 1e3) / 1e6
+    total_ms = max_over_ranks(total_ms, dist)
+    value = replica_throughput(pixels, world, args.steps, total_ms / 1e3) / 1e6
 
     ctx.set_tuning(use_graph=0)  # the batches below are decoded once each: nothing to replay
     # ---- plain per-image GPU path: one image per launch sequence
@@ -392,11 +406,8 @@ def run_serve(args, rank, world, dist):
         sat_s, bad = serve_pass(order)
         torch.cuda.synchronize()
     st1 = srv.stats()
-    if dist:
-        t = torch.tensor([sat_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        sat_s = float(t.item())
-    value = total_px * world / sat_s / 1e6
+    sat_s = max_over_ranks(sat_s, dist)
+    value = replica_throughput(total_px, world, 1, sat_s) / 1e6
 
     # ---- phase 2: Poisson arrivals
     rate = args.rate or 0.7 * n_req / sat_s
