@@ -441,27 +441,28 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
     uint8_t *rrow = b.rf + s * b.gap;
     for (int c0 = 0; c0 < b.w; c0 += 32) {
       __syncwarp();
-      // lane-parallel view of the chunk (unrolled form): each lane's word and the rows its
-      // pass would visit.  While decoding, a column's word changes only when its left
-      // neighbour gains a significant sample (`dirty`); the serial loop reloads those and
-      // uses the lanes' copies for the rest.  The compact form keeps fewer values live across
-      // the serial loop (registers bound its occupancy): it reloads every word and visits
-      // every column in cleanup.
+      // lane-parallel view of the chunk: each lane's word and the rows its pass would
+      // visit; only columns with work join the serial loop (a column reached from the left
+      // by a new significant sample joins it then).  The unrolled form also hands the
+      // lanes' words and masks to the serial loop: a column's word changes only when its
+      // left neighbour gains a significant sample (`dirty`), so only those are reloaded.
+      // The compact form keeps fewer values live across the serial loop (registers bound
+      // its occupancy) and reloads each word.
       constexpr bool LP = UNROLLED;
       const int c = c0 + lane;
       const bool valid = c < b.w;
       const uint32_t word = valid ? row[c] : 0u;
-      uint32_t mask = 0;
+      uint32_t mask;
       bool work;
       if (pass == P_SIGPROP) {
-        if (LP) mask = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(word);
-        work = LP ? mask != 0 : word != 0;
+        mask = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(word);
+        work = mask != 0;
       } else if (pass == P_MAGREF) {
-        if (LP) mask = row_mask<0u, V_SIG | V_MU, 0u>(word);
-        work = LP ? mask != 0 : (word & MU_ALL) != 0;
+        mask = row_mask<0u, V_SIG | V_MU, 0u>(word);
+        work = mask != 0;
       } else {
-        if (LP) mask = row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(word);
-        work = LP ? (word == 0 || mask != 0) : true;  // run mode, or rows not yet coded
+        mask = row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(word);
+        work = word == 0 || mask != 0;  // run mode, or rows not yet coded in this bit-plane
       }
       uint32_t live = __ballot_sync(0xffffffffu, valid && work);
       uint32_t zero = __ballot_sync(0xffffffffu, valid && word == 0);
@@ -510,10 +511,6 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
           const uint32_t todo =
               (dty && (!LP || lane_word == 0)) ? row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw) : lane_mask;
           newsig = cleanup_column<UNROLLED>(b, wp, cw, todo, 4 * s, col, p, zc, raw, mq, T);
-          if (!LP) {
-            cw |= (cw << (MU_POS - 4)) & MU_ALL;  // mu |= sigma, pi cleared
-            cw &= ~PI_ALL;
-          }
         }
         *wp = cw;
         if (newsig && bit < 31) {
@@ -522,7 +519,7 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
           if (LP) dirty |= 1u << (bit + 1);
         }
       }
-      if (LP && pass == P_CLEANUP) {
+      if (pass == P_CLEANUP) {
         // end of the bit-plane for this chunk's columns: mu |= sigma, pi cleared
         // (bmi_block_decoder.cpp:571-573); no later decision of this pass reads a column's
         // own mu / pi bits
