@@ -12,7 +12,8 @@ encoded and each appears 4 times in the batch (identical decode work per copy).
 One step = one decode of the whole batch.  `value` times steps with the coded bytes and
 work lists resident in HBM (CUDA events on the launch stream, L2 flushed between steps);
 `e2e` times the public C-ABI path from host memory: host Tier-2 of every frame,
-pinned H2D, decode, D2H of every decoded picture.  `--workload c5` runs the serving stream
+pinned H2D, decode, D2H of every decoded picture into pinned host buffers, with two contexts
+alternating so one step's host work overlaps the previous step's decode.  `--workload c5` runs the serving stream
 through the continuous-batching service instead (see run_serve).  Multi-GPU runs are replicas (each rank
 decodes its own copy of the batch; images are independent, no collective on the data path).
 """
@@ -253,24 +254,48 @@ def run_gpu(args, rank, world, dist):
             plain_ms.append((time.perf_counter() - t0) * 1e3)
     plain = sum(p.info.width * p.info.height for p in uniq) / (plain_ms[0] / 1e3) / 1e6
 
-    # ---- end to end through the C ABI with host buffers
-    outs = [np.empty(p.output_bytes(fmt), np.uint8) for p in plans]
+    # ---- end to end through the C ABI with host buffers.  Each step: host Tier-2 of every
+    # codestream, stage (pinned) + H2D, decode, D2H of every picture into pinned host
+    # buffers.  Two contexts alternate, so the host work and copies of one step overlap the
+    # device decode of the previous one, as a decoding service would run; the time is the
+    # wall clock from the first step's parse to the last step's pictures on the host.
+    import torch
+    ctx2 = native.GpuContext(dev)
+    ctxs = [ctx, ctx2]
+    e2e_streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    e2e_sp = [ctypes.c_void_p(x.cuda_stream) for x in e2e_streams]
+    outs = [[torch.empty(p.output_bytes(fmt), dtype=torch.uint8).pin_memory() for p in plans] for _ in range(2)]
     h2d = sum(p.info.coded_bytes for p in plans)
-    d2h = sum(o.nbytes for o in outs)
-    e2e_ms = []
-    for it in range(max(2, min(args.steps, 4)) + 1):
-        t0 = time.perf_counter()
-        ps = parse_all(streams, pool)
-        ctx.begin()
-        for p in ps:
-            ctx.add(p, fmt)
-        ctx.launch(sp)
-        assert ctx.sync() == 0
-        for i, o in enumerate(outs):
-            native.lib().j2k_gpu_output_copy(ctx.h, i, o.ctypes.data_as(ctypes.c_void_p), o.nbytes)
-        if it:
-            e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e = pixels * world / (float(np.median(e2e_ms)) / 1e3) / 1e6
+    d2h = sum(o.numel() for o in outs[0])
+
+    def collect(k):
+        assert ctxs[k].sync() == 0
+        for i, o in enumerate(outs[k]):
+            assert native.lib().j2k_gpu_output_copy(ctxs[k].h, i, ctypes.c_void_p(o.data_ptr()), o.numel()) == 0
+
+    def e2e_run(nsteps):
+        pending = None
+        for it in range(nsteps):
+            k = it % 2
+            ps = parse_all(streams, pool)
+            ctxs[k].begin()
+            for p in ps:
+                ctxs[k].add(p, fmt)
+            ctxs[k].launch(e2e_sp[k])
+            if pending is not None:
+                collect(pending)
+            pending = k
+        collect(pending)
+
+    e2e_run(2)  # warm: both contexts' pools and pinned buffers at size
+    n_e2e = max(2, min(args.steps, 6))
+    t0 = time.perf_counter()
+    e2e_run(n_e2e)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, dist)
+    e2e = replica_throughput(pixels, world, n_e2e, e2e_s) / 1e6
+    e2e_ms = [e2e_s * 1e3 / n_e2e]
+    ctx2.close()
 
     if rank != 0:
         return
@@ -306,7 +331,9 @@ def run_gpu(args, rank, world, dist):
             "config": cfg,
             "e2e": {"value": round(e2e, 2), "unit": "Mpixel/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": round(float(np.median(e2e_ms)), 3),
-                    "includes": "host Tier-2 parse + pinned H2D + decode + D2H of every picture"},
+                    "includes": "per step: host Tier-2 of every codestream, staging + H2D, decode, D2H of every "
+                                "picture into pinned host buffers; two contexts alternate so one step's host "
+                                "work overlaps the previous step's decode (wall clock over the steps)"},
             "plain_gpu_path": {"value": round(plain, 2), "unit": "Mpixel/s", "images": len(uniq),
                                "what": "one image per launch sequence, host buffers"},
             "speedup_vs_plain": round(value / plain, 2),
