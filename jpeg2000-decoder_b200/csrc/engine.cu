@@ -691,11 +691,17 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       }
     }
   }
-  // work queue order: longest coded length first
-  auto by_len = [&](uint32_t a, uint32_t b) { return cbs[a].data_len > cbs[b].data_len; };
+  // work queue order: longest coded length first (counting sort on the length in 16-byte
+  // steps, capped at 64 KB: linear time; order within a step is irrelevant to the queue)
   size_t n_ord = 0;
   for (auto &q : ordq) {
-    std::sort(q.begin(), q.end(), by_len);
+    constexpr int NB = 4096;
+    std::vector<uint32_t> cnt(NB + 1, 0), tmp(q.size());
+    auto key = [&](uint32_t i) { return NB - 1 - (int)(std::min<uint32_t>(cbs[i].data_len, 65535u) >> 4); };
+    for (uint32_t i : q) cnt[key(i) + 1]++;
+    for (int b = 0; b < NB; ++b) cnt[b + 1] += cnt[b];
+    for (uint32_t i : q) tmp[cnt[key(i)]++] = i;
+    q.swap(tmp);
     n_ord += q.size();
   }
   std::vector<uint32_t> dtask_off(2 * maxL + 1, 0);
@@ -750,11 +756,25 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::memcpy(H + o_ftk, ftasks[0].data(), ftasks[0].size() * sizeof(OutTask));
   std::memcpy(H + o_ftk + ftasks[0].size() * sizeof(OutTask), ftasks[1].data(), ftasks[1].size() * sizeof(OutTask));
   {
+    // coded bytes of every image, copied by a few threads when there are many
+    std::vector<std::pair<size_t, const std::vector<uint8_t> *>> parts;
     size_t off = o_byt;
     for (auto &im : c->imgs) {
-      const auto &b = im.plan->p.bytes;
-      if (!b.empty()) std::memcpy(H + off, b.data(), b.size());
-      off += b.size();
+      parts.push_back({off, &im.plan->p.bytes});
+      off += im.plan->p.bytes.size();
+    }
+    auto copy_range = [&](size_t lo, size_t hi) {
+      for (size_t k = lo; k < hi; ++k)
+        if (!parts[k].second->empty()) std::memcpy(H + parts[k].first, parts[k].second->data(), parts[k].second->size());
+    };
+    const size_t nt = S.bytes > (8u << 20) ? std::min<size_t>(8, parts.size()) : 1;
+    if (nt <= 1) {
+      copy_range(0, parts.size());
+    } else {
+      std::vector<std::thread> th;
+      for (size_t t = 0; t < nt; ++t)
+        th.emplace_back(copy_range, parts.size() * t / nt, parts.size() * (t + 1) / nt);
+      for (auto &x : th) x.join();
     }
   }
 
