@@ -194,16 +194,27 @@ __device__ __forceinline__ void dwt_windows(DwtSmem<REV> *S, int nw, const WinSr
   // issues all of its loads before waiting, so a CTA has all its windows in flight;
   // consecutive threads read consecutive source columns
   constexpr int QN = DWT_N / 2;  // 36 window lines of each parity
+  // a warp copies one quadrant row at a time; each lane holds the source columns of
+  // quadrant columns j = lane and (lanes 0..3) j = lane + 32, for both parities
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const bool two = lane < QN - 32;
+  const int sc_e0 = S[0].scol[2 * lane], sc_o0 = S[0].scol[2 * lane + 1];
+  const int sc_e1 = two ? S[0].scol[2 * (lane + 32)] : 0, sc_o1 = two ? S[0].scol[2 * (lane + 32) + 1] : 0;
   for (int w = 0; w < nw; ++w) {
     const uint32_t tile_s = (uint32_t)__cvta_generic_to_shared(S[w].tile);
     const WinSrc<REV> in = src[w];
-    for (int e = threadIdx.x; e < 4 * QN * QN; e += blockDim.x) {
-      const int qd = e / (QN * QN), r = (e - qd * QN * QN) / QN, j = e - qd * QN * QN - r * QN;
-      const int iy = 2 * r + (qd >> 1), ix = 2 * j + (qd & 1);
-      const T *p = qd == 0 ? in.llsrc + (size_t)S[0].srow[iy] * in.stride_ll + S[0].scol[ix]
-                           : in.quad + (size_t)S[0].srow[iy] * in.stride_q + S[0].scol[ix];
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(tile_s + 4u * (iy * DWT_PITCH + ix)), "l"(p)
+    for (int rr = warp; rr < 4 * QN; rr += nwarps) {
+      const int qd = rr / QN, r = rr - qd * QN;  // quadrant (LL, HL, LH, HH) and its row
+      const int iy = 2 * r + (qd >> 1), odd = qd & 1;
+      const T *line = qd == 0 ? in.llsrc + (size_t)S[0].srow[iy] * in.stride_ll
+                              : in.quad + (size_t)S[0].srow[iy] * in.stride_q;
+      const uint32_t dst = tile_s + 4u * (iy * DWT_PITCH + odd);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8u * lane), "l"(line + (odd ? sc_o0 : sc_e0))
                    : "memory");
+      if (two)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8u * (lane + 32)),
+                     "l"(line + (odd ? sc_o1 : sc_e1))
+                     : "memory");
     }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -341,6 +352,26 @@ struct FusedGroup {
   int32_t stride, rw, rh, lw, lh;
 };
 
+// Inverse RCT (5/3, int) or ICT (9/7, float) + DC level shift + clamp of one pixel: R, G, B
+// (RRct_53 :3936-4130, RICT_97_FLOAT :3570-3643 of bmi_cpu_dwt_decoder.cpp)
+template <typename T>
+__device__ __forceinline__ void mct_pixel(T y, T u, T w, int dc, int maxv, int *rgb) {
+  if constexpr (std::is_integral<T>::value) {
+    const int g = (int)y - (((int)u + (int)w) >> 2) + dc;
+    rgb[0] = clampi((int)w + g, maxv);
+    rgb[1] = clampi(g, maxv);
+    rgb[2] = clampi((int)u + g, maxv);
+  } else {
+    const float sh = (float)dc, fm = (float)maxv;
+    float t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.402f, w)), sh);
+    rgb[0] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+    t = __fadd_rn(__fadd_rn(__fadd_rn(y, __fmul_rn(-0.34413f, u)), __fmul_rn(-0.71414f, w)), sh);
+    rgb[1] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+    t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.772f, u)), sh);
+    rgb[2] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
+  }
+}
+
 // Inverse RCT / ICT + DC level shift + clamp + LIFT + pack of one pixel (bmi_cpu_dwt_decoder.cpp
 // RICT_97_FLOAT :3570-3643, RRct_53 :3936-4130, MergeComponents :4283-4598).  `v[c]` is
 // component c's reconstructed sample (int32 for 5/3, float for 9/7), `have[c]` whether the
@@ -360,22 +391,7 @@ __device__ __forceinline__ void emit_pixel(const OutGroup &G, uint8_t *out, int 
   uint8_t tmp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (do_mct) {
     int c3[3];
-    if constexpr (INT) {
-      const int y = v[0], u = v[1], w = v[2];
-      const int g = y - ((u + w) >> 2) + dc;
-      c3[0] = clampi(w + g, maxv);
-      c3[1] = clampi(g, maxv);
-      c3[2] = clampi(u + g, maxv);
-    } else {
-      const float y = v[0], u = v[1], w = v[2];
-      const float sh = (float)dc, fm = (float)maxv;
-      float t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.402f, w)), sh);
-      c3[0] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
-      t = __fadd_rn(__fadd_rn(__fadd_rn(y, __fmul_rn(-0.34413f, u)), __fmul_rn(-0.71414f, w)), sh);
-      c3[1] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
-      t = __fadd_rn(__fadd_rn(y, __fmul_rn(1.772f, u)), sh);
-      c3[2] = (int)(t < 0.f ? 0.f : (t > fm ? fm : t));
-    }
+    mct_pixel<T>(v[0], v[1], v[2], dc, maxv, c3);
     if (G.checkout >= 0 && G.checkout < 3) {
       // one component replicated into R, G and B (RICT_97_FLOAT / RRct_53 case 0..2)
       const int vv = lift_depth(c3[G.checkout], B, outdepth);
@@ -464,12 +480,41 @@ __global__ void __launch_bounds__(FUSED_THREADS) last_level_output_kernel(const 
     const int ox = tk.tx * DWT_T, oy = tk.ty * DWT_T;
     dwt_windows<REV>(S, nc, src, F.rw, F.rh, F.lw, F.lh, F.ll_gain != 0, ll_gain_value, F.refcompat != 0, ox, oy);
     const int ow = min(DWT_T, F.rw - ox), oh = min(DWT_T, F.rh - oy);
-    for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
-      const int yy = i / DWT_T, xx = i % DWT_T;
-      if (yy >= oh || xx >= ow) continue;
-      T v[4] = {0, 0, 0, 0};
-      for (int c = 0; c < nc; ++c) v[c] = S[c].tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
-      emit_pixel<T>(G, out, oy + yy, ox + xx, v, have);
+    if (G.fmt == 2 && G.bitdepth == 8 && G.mct && nc == 3) {
+      // 24-bit RGB after the inverse MCT (the common path): four pixels per thread, stored
+      // as three 32-bit words when the row allows (bytes B, G, R per pixel)
+      for (int i = threadIdx.x; i < DWT_T * (DWT_T / 4); i += blockDim.x) {
+        const int yy = i / (DWT_T / 4), xx = (i % (DWT_T / 4)) * 4;
+        if (yy >= oh || xx >= ow) continue;
+        uint8_t *px = out + G.out_off + ((size_t)(G.y0 + oy + yy) * G.pitch_px + (G.x0 + ox + xx)) * 3;
+        uint32_t bytes[3] = {0, 0, 0};
+        const int npx = min(4, ow - xx);
+        for (int k = 0; k < 4; ++k) {
+          const int o = (yy + DWT_H) * DWT_PITCH + xx + k + DWT_H;
+          int rgb[3];
+          mct_pixel<T>(S[0].tile[o], S[1].tile[o], S[2].tile[o], 128, 255, rgb);
+          for (int j = 0; j < 3; ++j) {
+            const int b = k * 3 + j;  // byte j of pixel k: B, G, R
+            bytes[b >> 2] |= (uint32_t)rgb[2 - j] << (8 * (b & 3));
+          }
+        }
+        if (npx == 4 && !((uintptr_t)px & 3)) {
+          uint32_t *w = reinterpret_cast<uint32_t *>(px);
+          w[0] = bytes[0];
+          w[1] = bytes[1];
+          w[2] = bytes[2];
+        } else {
+          for (int b = 0; b < npx * 3; ++b) px[b] = (uint8_t)(bytes[b >> 2] >> (8 * (b & 3)));
+        }
+      }
+    } else {
+      for (int i = threadIdx.x; i < DWT_T * DWT_T; i += blockDim.x) {
+        const int yy = i / DWT_T, xx = i % DWT_T;
+        if (yy >= oh || xx >= ow) continue;
+        T v[4] = {0, 0, 0, 0};
+        for (int c = 0; c < nc; ++c) v[c] = S[c].tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
+        emit_pixel<T>(G, out, oy + yy, ox + xx, v, have);
+      }
     }
     __syncthreads();
   }
