@@ -150,21 +150,38 @@ __device__ __forceinline__ void mq_renorm(Mq &m) {
 
 // MQ_DECODE, bmi_mq_decoder.h:86-128, on a context slot holding its table entry.  Both
 // renormalising outcomes (conditional exchange after C < Qe; A below 0x8000 after C >= Qe)
-// share one table update and one renormalisation.
+// share one table update and one renormalisation.  EARLY (compact kernel form: fewest
+// instructions) returns the common outcome first: C >= Qe and A still >= 0x8000 after
+// A -= Qe (MPS, no renormalisation); otherwise (unrolled form: shortest dependency chain)
+// the outcome is computed before a single branch.
+template <bool EARLY>
 __device__ __forceinline__ int mq_decode(Mq &m, uint2 *cx, const uint2 *tab) {
   const uint2 e = *cx;
   const int32_t q = (int32_t)e.x;
   m.A -= q;
   const bool ex = m.C < q;
-  const bool lps = ex ? (m.A >= q) : (m.A < q);
-  const int sym = (int)((e.y >> 16) & 1) ^ (int)lps;
-  if (!ex) m.C -= q;
-  if (ex || m.A < 0x800000) {
-    *cx = tab[lps ? (e.y & 0xFF) : ((e.y >> 8) & 0xFF)];
+  if constexpr (EARLY) {
+    if (!ex && m.A >= 0x800000) {
+      m.C -= q;
+      return (int)((e.y >> 16) & 1);
+    }
+    const bool lps = (m.A < q) != ex;
     if (ex) m.A = q;
+    else m.C -= q;
+    *cx = tab[lps ? (e.y & 0xFF) : ((e.y >> 8) & 0xFF)];
     mq_renorm(m);
+    return (int)((e.y >> 16) & 1) ^ (int)lps;
+  } else {
+    const bool lps = ex ? (m.A >= q) : (m.A < q);
+    const int sym = (int)((e.y >> 16) & 1) ^ (int)lps;
+    if (!ex) m.C -= q;
+    if (ex || m.A < 0x800000) {
+      *cx = tab[lps ? (e.y & 0xFF) : ((e.y >> 8) & 0xFF)];
+      if (ex) m.A = q;
+      mq_renorm(m);
+    }
+    return sym;
   }
-  return sym;
 }
 
 // MQ_DECODE_START (fixed Qe 0x5601, MPS 0, no adaptation), bmi_mq_decoder.h:131-169
@@ -288,12 +305,14 @@ __device__ __forceinline__ void spread_sig(const BlockSmem &b, uint32_t *wp, uin
 enum { P_SIGPROP = 0, P_MAGREF = 1, P_CLEANUP = 2 };
 
 // one decision: a raw bit in a bypass segment, else an MQ symbol
+template <bool UNROLLED>
 __device__ __forceinline__ int decide(bool israw, Raw &raw, Mq &mq, uint2 *slot, const uint2 *tab) {
-  return israw ? raw_bit(raw) : mq_decode(mq, slot, tab);
+  return israw ? raw_bit(raw) : mq_decode<!UNROLLED>(mq, slot, tab);
 }
 
 // Sign of row k (raw bit, or MQ symbol in the sign context of its neighbours XOR the
 // context's prediction bit), then the sample becomes significant
+template <bool UNROLLED>
 __device__ __forceinline__ void significant(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int k, int col,
                                             int p, bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
   int flip = 0, slot = C_SIGN;
@@ -302,7 +321,7 @@ __device__ __forceinline__ void significant(const BlockSmem &b, uint32_t *wp, ui
     slot += sv >> 1;
     flip = sv & 1;
   }
-  const int sg = decide(israw, raw, mq, b.cx + slot, T.mq) ^ flip;
+  const int sg = decide<UNROLLED>(israw, raw, mq, b.cx + slot, T.mq) ^ flip;
   spread_sig(b, wp, cw, k, sg);
   b.sp.set_sig(row + k, col, sg, p);
 }
@@ -344,10 +363,10 @@ __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp,
     for (int k = 0; k < 4; ++k) {
       const uint32_t v = cw >> (3 * k);
       if (!(v & NBR_ROW0) || (v & (V_SIG | V_CHI))) continue;
-      const int d = decide(israw, raw, mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq);
+      const int d = decide<UNROLLED>(israw, raw, mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq);
       cw |= ROW_PI(k);
       if (d) {
-        significant(b, wp, cw, row, k, col, p, israw, raw, mq, T);
+        significant<UNROLLED>(b, wp, cw, row, k, col, p, israw, raw, mq, T);
         newsig = true;
       }
     }
@@ -355,10 +374,10 @@ __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp,
     while (todo) {
       const int k = __ffs(todo) - 1;
       todo &= todo - 1;
-      const int d = decide(israw, raw, mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
+      const int d = decide<UNROLLED>(israw, raw, mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
       cw |= ROW_PI(k);
       if (d) {
-        significant(b, wp, cw, row, k, col, p, israw, raw, mq, T);
+        significant<UNROLLED>(b, wp, cw, row, k, col, p, israw, raw, mq, T);
         newsig = true;
         todo = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw) & (0xEu << k);
       }
@@ -381,7 +400,7 @@ __device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, u
       todo &= todo - 1;
       // first refinement of this sample <=> (|v| >> p) < 4 in the reference
       const int ctx = C_MAG + (((refined >> k) & 1) ? 2 : (((cw >> (3 * k)) & NBR_ROW0) ? 1 : 0));
-      const int d = decide(israw, raw, mq, b.cx + ctx, T.mq);
+      const int d = decide<UNROLLED>(israw, raw, mq, b.cx + ctx, T.mq);
       b.sp.refine(row + k, col, d, p);
     }
   }
@@ -403,7 +422,7 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
     int r = 0;
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
-      const int d = mq_decode(mq, b.cx + (i == 0 ? C_RUN : C_UNI), T.mq);
+      const int d = mq_decode<!UNROLLED>(mq, b.cx + (i == 0 ? C_RUN : C_UNI), T.mq);
       if (i == 0 && !d) return false;  // the whole column stays insignificant
       r = (r << 1) | d;
     }
@@ -417,8 +436,8 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
     while (rows) {
       const int k = UNROLLED ? i : __ffs(rows) - 1;
       rows &= rows - 1;
-      if (k != forced && !mq_decode(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq)) continue;
-      significant(b, wp, cw, row, k, col, p, false, raw, mq, T);
+      if (k != forced && !mq_decode<!UNROLLED>(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq)) continue;
+      significant<UNROLLED>(b, wp, cw, row, k, col, p, false, raw, mq, T);
       newsig = true;
     }
   }
