@@ -151,7 +151,10 @@ def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
         oracle_util.oracle_decode(p, f)
         return p.info.width * p.info.height
 
+    orc = oracle_util.orc()
+    orc.oracle_decisions.restype = ctypes.c_ulonglong
     with ThreadPoolExecutor(max_workers=threads) as ex:
+        d0 = orc.oracle_decisions()
         t0 = time.perf_counter()
         px = 0
         rounds = 0
@@ -161,7 +164,12 @@ def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
             if time.perf_counter() - t0 > budget_s or rounds >= 8:
                 break
         dt = time.perf_counter() - t0
+        decisions_per_px = (orc.oracle_decisions() - d0) / max(1, px)
+    cpu_decode_sample.decisions_per_px = decisions_per_px
     return px / dt / 1e6, threads, "%d image decodes (%d distinct) in %.1f s" % (rounds * len(plans), len(plans), dt)
+
+
+cpu_decode_sample.decisions_per_px = None
 
 
 def run_reference_arm(args, rank, world):
@@ -319,6 +327,14 @@ def run_gpu(args, rank, world, dist):
                 "kernel": "dwt_level_kernel + output_kernel", "peak_source": peak_kind,
                 "algorithmic_bytes": dwt_bytes, "ms_per_step": round(dwt_ms, 4)}
     cpu_v, cores, sample = cpu_decode_sample(streams, fmt, budget_s=args.cpu_budget)
+    dpp = cpu_decode_sample.decisions_per_px
+    if dpp:
+        # Tier-1 work rate: decisions of the standard decoding process (MQ symbols incl. run
+        # and uniform ones, raw bits; counted by the CPU restatement on the sample, whose
+        # pictures are those of the batch) and compressed bytes per second of Tier-1 time
+        roof_t1["decisions_per_s"] = round(dpp * pixels / (t1_ms / 1e3), 1)
+        roof_t1["decisions_per_px"] = round(dpp, 3)
+    roof_t1["compressed_bytes_per_s"] = round(coded / (t1_ms / 1e3), 1)
     clocks = clk.summary()
     cfg = dict(cfg)
     cfg.update({"parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",

@@ -95,7 +95,13 @@ static void mq_renorm_once(mq_t *m) {
   m->t--;
 }
 
+/* Decisions decoded (MQ symbols and raw bits), counted per thread and added to a process
+ * total at the end of each block: a workload statistic for the benchmark report. */
+static _Thread_local unsigned long long t_decisions;
+static unsigned long long g_decisions;
+
 static int mq_decode(mq_t *m, ctx_t *cx) {
+  t_decisions++;
   int32_t q = (int32_t)QE[cx->idx] << 8;
   int ret = cx->mps;
   int sw = (QE[cx->idx] == 0x5601 && NLPS[cx->idx] != 46);
@@ -130,6 +136,7 @@ static int mq_decode(mq_t *m, ctx_t *cx) {
 
 /* fixed-probability (Qe 0x5601, MPS 0) symbol: bmi_mq_decoder.h:131-169 (MQ_DECODE_START) */
 static int mq_decode_uniform(mq_t *m) {
+  t_decisions++;
   int ret = 0;
   if (m->C < 0x560100) {
     if (m->A >= (0x560100 << 1)) ret = 1;
@@ -168,6 +175,7 @@ static void raw_init(raw_t *r, const uint8_t *buf, uint32_t len) {
   r->last = 0;
 }
 static int raw_bit(raw_t *r) {
+  t_decisions++;
   if (r->ct == 0) {
     int b = r->p < r->end ? *r->p : 0xFF;
     r->p++;
@@ -405,7 +413,18 @@ static int seg_starts(int flags, int j) {
   return (flags & J2K_CB_BYPASS) && j >= 10 && type != 1;
 }
 
+unsigned long long oracle_decisions(void) { return __atomic_load_n(&g_decisions, __ATOMIC_RELAXED); }
+
+static int t1_block(const j2k_cblk *cb, const uint8_t *bytes, const uint32_t *seglens, int32_t *out);
+
 int oracle_t1_block(const j2k_cblk *cb, const uint8_t *bytes, const uint32_t *seglens, int32_t *out) {
+  t_decisions = 0;
+  const int rc = t1_block(cb, bytes, seglens, out);
+  __atomic_fetch_add(&g_decisions, t_decisions, __ATOMIC_RELAXED);
+  return rc;
+}
+
+static int t1_block(const j2k_cblk *cb, const uint8_t *bytes, const uint32_t *seglens, int32_t *out) {
   const int w = cb->w, h = cb->h;
   const int stripes = (h + 3) >> 2;
   const int irrev = (cb->flags & J2K_CB_IRREV) != 0;

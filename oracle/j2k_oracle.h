@@ -28,6 +28,9 @@ enum {
 /* Tier-1 of one code-block: w*h int32 samples in the reference's raw form
  * (bit 31 sign, magnitude with midpoint bits).  Returns 0 or an error status. */
 int oracle_t1_block(const j2k_cblk *cb, const uint8_t *bytes, const uint32_t *seglens, int32_t *out);
+/* Tier-1 decisions (MQ symbols incl. run-length and uniform ones, raw bits) decoded so far
+ * by this process: a workload statistic for the benchmark report. */
+unsigned long long oracle_decisions(void);
 /* Tier-1 of all blocks placed into the coefficient buffer (int32 for 5/3, float for 9/7). */
 int oracle_t1_place(const j2k_cblk *cblks, int ncb, const uint8_t *bytes, const uint32_t *seglens, void *coef,
                     int32_t *status);
