@@ -314,3 +314,27 @@ def test_fused_last_level_equals_kept_components_path(gpu_ctx, name):
             with pytest.raises(native.J2kError):
                 gpu_ctx.component(0, 0)
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("h,w", [(1, 1), (1, 7), (5, 1), (3, 5), (17, 1), (1, 33), (2, 2), (65, 63), (7, 130), (129, 3)])
+def test_tiny_and_odd_geometries_bit_exact(gpu_ctx, h, w):
+    """Pictures smaller than a code-block, one sample wide or high, odd sizes, more DWT
+    levels than the size supports: every Tier-1 and DWT edge path, 5/3 and 9/7, one and
+    three components, both Tier-1 kernel forms; GPU equals the oracle (tolerance 0), and
+    5/3 equals its source."""
+    from jpeg2000_decoder_b200 import native
+    rng = np.random.default_rng(h * 1000 + w)
+    for rev in (1, 0):
+        for ncomp in (1, 3):
+            img = rng.integers(0, 256, (ncomp, h, w)).astype(np.uint16)
+            cs = native.encode(img, 8, reversible=rev, levels=5, cbw_exp=6, cbh_exp=6, num_layers=1,
+                               layer_bpp=[0 if rev else 4.0], guard_bits=2 if rev else 1)
+            fmt = native.FMT_32BITS_4COMPONENTS if ncomp == 1 else native.FMT_24BITS_RGB
+            for form in (1, 2):
+                gpu_ctx.set_tuning(t1_form=form)
+                out, _ = _decode_check(gpu_ctx, cs, fmt)
+                if rev:
+                    px = (out.reshape(h, w, 3)[:, :, ::-1].transpose(2, 0, 1) if ncomp == 3
+                          else out.reshape(h, w, 4)[:, :, 3][None])
+                    assert np.array_equal(px, img)
+    gpu_ctx.set_tuning()
