@@ -44,9 +44,6 @@
 
 #include "plan.h"
 
-#ifndef J2K_T1_RED_VARIANT
-#define J2K_T1_RED_VARIANT 0
-#endif
 
 
 namespace j2k_dev {
@@ -232,30 +229,29 @@ __device__ __forceinline__ int raw_bit(Raw &r) {
 }
 
 // ---- samples: raw int32 (bit 31 sign, magnitude with midpoint bit) accumulated in global
-// memory by XOR updates from lane 0; the block region is zeroed before decoding
+// memory by XOR updates; the block region is zeroed before decoding.  The updates of one
+// stripe column are collected while it is decoded and issued together at its end, one
+// fire-and-forget atomic per row from lanes 0..3 in a single warp instruction (nothing reads
+// the samples while decoding, and XOR updates commute).
 struct Samples {
   int32_t *base;      // the block's first sample in the output buffer
   uint32_t stride;    // elements per row
   int lane;
-  // one reduction issued by lane 0; the warp does not wait for it
-  __device__ __forceinline__ void xor_at(int row, int col, uint32_t v) const {
-    unsigned int *a = reinterpret_cast<unsigned int *>(base + (size_t)row * stride + col);
-#if J2K_T1_RED_VARIANT == 0
-    if (lane == 0) atomicXor(a, v);
-#elif J2K_T1_RED_VARIANT == 1
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.eq.s32 p, %2, 0;\n\t@p red.relaxed.gpu.global.xor.b32 [%0], %1;\n\t}" ::"l"(a),
-                 "r"(v), "r"(lane)
-                 : "memory");
-#else
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.eq.s32 p, %2, 0;\n\t@p red.relaxed.gpu.global.xor.b32 [%0], %1;\n\t}" ::"l"(a),
-                 "r"(v), "r"(lane));
-#endif
+  // column update: bits 0..3 rows updated, bits 4..7 the sign (significance) or the
+  // decoded refinement bit of each row
+  __device__ __forceinline__ void apply_sig(int row0, int col, uint32_t upd, int plane) const {
+    if (lane < 4 && ((upd >> lane) & 1)) {
+      const uint32_t sign = (upd >> (4 + lane)) & 1;
+      atomicXor(reinterpret_cast<unsigned int *>(base + (size_t)(row0 + lane) * stride + col),
+                (sign << 31) + (1u << plane) + ((1u << plane) >> 1));
+    }
   }
-  __device__ __forceinline__ void set_sig(int row, int col, int sign, int plane) const {
-    xor_at(row, col, ((uint32_t)sign << 31) + (1u << plane) + ((1u << plane) >> 1));
-  }
-  __device__ __forceinline__ void refine(int row, int col, int sym, int plane) const {
-    xor_at(row, col, ((uint32_t)(1 - sym) << plane) | ((1u << plane) >> 1));
+  __device__ __forceinline__ void apply_ref(int row0, int col, uint32_t upd, int plane) const {
+    if (lane < 4 && ((upd >> lane) & 1)) {
+      const uint32_t sym = (upd >> (4 + lane)) & 1;
+      atomicXor(reinterpret_cast<unsigned int *>(base + (size_t)(row0 + lane) * stride + col),
+                ((1u - sym) << plane) | ((1u << plane) >> 1));
+    }
   }
 };
 
@@ -311,10 +307,10 @@ __device__ __forceinline__ int decide(bool israw, Raw &raw, Mq &mq, uint2 *slot,
 }
 
 // Sign of row k (raw bit, or MQ symbol in the sign context of its neighbours XOR the
-// context's prediction bit), then the sample becomes significant
+// context's prediction bit), then the sample becomes significant; returns its column update
 template <bool UNROLLED>
-__device__ __forceinline__ void significant(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int row, int k, int col,
-                                            int p, bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
+__device__ __forceinline__ uint32_t significant(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, bool israw,
+                                                Raw &raw, Mq &mq, const T1Tables &T) {
   int flip = 0, slot = C_SIGN;
   if (!israw) {
     const int sv = T.sc[sign_index(cw, wp[-1], wp[1], k)];
@@ -323,7 +319,7 @@ __device__ __forceinline__ void significant(const BlockSmem &b, uint32_t *wp, ui
   }
   const int sg = decide<UNROLLED>(israw, raw, mq, b.cx + slot, T.mq) ^ flip;
   spread_sig(b, wp, cw, k, sg);
-  b.sp.set_sig(row + k, col, sg, p);
+  return (1u << k) | ((uint32_t)sg << (4 + k));  // this row's column update
 }
 
 // Rows of a stripe column that pass a pass's test, as a 4-bit mask (bit k = row k), with
@@ -354,10 +350,10 @@ constexpr uint32_t V_SIG = 0x10u, V_CHI = 1u << CHI_POS, V_MU = 1u << MU_POS, V_
 // not yet significant with a significant neighbour; a row that becomes significant can
 // make the rows below it eligible
 template <bool UNROLLED>
-__device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, uint32_t todo, int row,
-                                               int col, int p, bool israw, const uint8_t *zc, Raw &raw, Mq &mq,
-                                               const T1Tables &T) {
-  bool newsig = false;
+__device__ __forceinline__ uint32_t sigprop_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, uint32_t todo,
+                                                   bool israw, const uint8_t *zc, Raw &raw, Mq &mq,
+                                                   const T1Tables &T) {
+  uint32_t upd = 0;
   if constexpr (UNROLLED) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -365,10 +361,7 @@ __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp,
       if (!(v & NBR_ROW0) || (v & (V_SIG | V_CHI))) continue;
       const int d = decide<UNROLLED>(israw, raw, mq, b.cx + C_SIG + zc[v & NBR_ROW0], T.mq);
       cw |= ROW_PI(k);
-      if (d) {
-        significant<UNROLLED>(b, wp, cw, row, k, col, p, israw, raw, mq, T);
-        newsig = true;
-      }
+      if (d) upd |= significant<UNROLLED>(b, wp, cw, k, israw, raw, mq, T);
     }
   } else {
     while (todo) {
@@ -377,21 +370,21 @@ __device__ __forceinline__ bool sigprop_column(const BlockSmem &b, uint32_t *wp,
       const int d = decide<UNROLLED>(israw, raw, mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq);
       cw |= ROW_PI(k);
       if (d) {
-        significant<UNROLLED>(b, wp, cw, row, k, col, p, israw, raw, mq, T);
-        newsig = true;
+        upd |= significant<UNROLLED>(b, wp, cw, k, israw, raw, mq, T);
         todo = row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw) & (0xEu << k);
       }
     }
   }
-  return newsig;
+  return upd;
 }
 
 // magnitude refinement of one stripe column (bmi_block_decoder.cpp:217-349): rows
 // significant before this bit-plane
 template <bool UNROLLED>
-__device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, uint32_t rows, uint8_t *rf, int row,
-                                              int col, int p, bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
+__device__ __forceinline__ uint32_t magref_column(const BlockSmem &b, uint32_t cw, uint32_t rows, uint8_t *rf,
+                                                  bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
   const uint32_t refined = *rf;
+  uint32_t bits = 0;
 #pragma unroll
   for (int i = 0; i < (UNROLLED ? 4 : 1); ++i) {
     uint32_t todo = UNROLLED ? (rows & (1u << i)) : rows;
@@ -400,11 +393,11 @@ __device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, u
       todo &= todo - 1;
       // first refinement of this sample <=> (|v| >> p) < 4 in the reference
       const int ctx = C_MAG + (((refined >> k) & 1) ? 2 : (((cw >> (3 * k)) & NBR_ROW0) ? 1 : 0));
-      const int d = decide<UNROLLED>(israw, raw, mq, b.cx + ctx, T.mq);
-      b.sp.refine(row + k, col, d, p);
+      bits |= (uint32_t)decide<UNROLLED>(israw, raw, mq, b.cx + ctx, T.mq) << (4 + k);
     }
   }
   if (rows) *rf = (uint8_t)(refined | rows);
+  return rows | bits;  // column update: rows refined and their decoded bits
 }
 
 // cleanup of one stripe column (bmi_block_decoder.cpp:351-586): an all-zero column is
@@ -412,9 +405,8 @@ __device__ __forceinline__ void magref_column(const BlockSmem &b, uint32_t cw, u
 // of the first significant sample, whose sign follows directly); then every row not yet
 // coded in this bit-plane
 template <bool UNROLLED>
-__device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, uint32_t todo, int row,
-                                               int col, int p, const uint8_t *zc, Raw &raw, Mq &mq,
-                                               const T1Tables &T) {
+__device__ __forceinline__ uint32_t cleanup_column(const BlockSmem &b, uint32_t *wp, uint32_t &cw, uint32_t todo,
+                                                   const uint8_t *zc, Raw &raw, Mq &mq, const T1Tables &T) {
   int forced = -1;
   if (cw == 0) {
     // run-length symbol, then the two uniform symbols (the reference's fixed-Qe
@@ -423,13 +415,13 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
 #pragma unroll 1
     for (int i = 0; i < 3; ++i) {
       const int d = mq_decode<!UNROLLED>(mq, b.cx + (i == 0 ? C_RUN : C_UNI), T.mq);
-      if (i == 0 && !d) return false;  // the whole column stays insignificant
+      if (i == 0 && !d) return 0;  // the whole column stays insignificant
       r = (r << 1) | d;
     }
     forced = r & 3;
     todo = (0xFu << forced) & 0xFu;
   }
-  bool newsig = false;
+  uint32_t upd = 0;
 #pragma unroll
   for (int i = 0; i < (UNROLLED ? 4 : 1); ++i) {
     uint32_t rows = UNROLLED ? (todo & (1u << i)) : todo;
@@ -437,11 +429,10 @@ __device__ __forceinline__ bool cleanup_column(const BlockSmem &b, uint32_t *wp,
       const int k = UNROLLED ? i : __ffs(rows) - 1;
       rows &= rows - 1;
       if (k != forced && !mq_decode<!UNROLLED>(mq, b.cx + C_SIG + zc[(cw >> (3 * k)) & NBR_ROW0], T.mq)) continue;
-      significant<UNROLLED>(b, wp, cw, row, k, col, p, false, raw, mq, T);
-      newsig = true;
+      upd |= significant<UNROLLED>(b, wp, cw, k, false, raw, mq, T);
     }
   }
-  return newsig;
+  return upd;
 }
 
 // One coding pass over the block.  Columns are visited in 32-column chunks: a ballot
@@ -517,21 +508,24 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
         }
         if (pass == P_MAGREF) {
           const uint32_t rows = LP ? lane_mask : row_mask<0u, V_SIG | V_MU, 0u>(cw);
-          magref_column<UNROLLED>(b, cw, rows, rrow + col, 4 * s, col, p, israw, raw, mq, T);
+          const uint32_t upd = magref_column<UNROLLED>(b, cw, rows, rrow + col, israw, raw, mq, T);
+          b.sp.apply_ref(4 * s, col, upd, p);
           continue;
         }
-        bool newsig;
+        uint32_t upd;
         if (pass == P_SIGPROP) {
           const uint32_t todo = dty ? row_mask<V_SIG | V_CHI, 0u, NBR_ROW0>(cw) : lane_mask;
-          newsig = sigprop_column<UNROLLED>(b, wp, cw, todo, 4 * s, col, p, israw, zc, raw, mq, T);
+          upd = sigprop_column<UNROLLED>(b, wp, cw, todo, israw, zc, raw, mq, T);
         } else {
           // own-row bits do not change from the left, so the lane's mask holds; a column
           // that was all-zero may have been reached from the left and is not any more
           const uint32_t todo =
               (dty && (!LP || lane_word == 0)) ? row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw) : lane_mask;
-          newsig = cleanup_column<UNROLLED>(b, wp, cw, todo, 4 * s, col, p, zc, raw, mq, T);
+          upd = cleanup_column<UNROLLED>(b, wp, cw, todo, zc, raw, mq, T);
         }
         *wp = cw;
+        const bool newsig = (upd & 0xF) != 0;
+        if (newsig) b.sp.apply_sig(4 * s, col, upd, p);
         if (newsig && bit < 31) {
           if (pass == P_SIGPROP) live |= 1u << (bit + 1);
           zero &= ~(1u << (bit + 1));
