@@ -165,6 +165,15 @@ void build_t1_tables(T1Tables &T) {
     T.mq[s].x = (uint32_t)QE[idx] << 8;
     T.mq[s].y = ((uint32_t)mps << 16) | (nm << 8) | nl;
   }
+  for (int r = 0; r < 16; ++r) {
+    const int n = __builtin_popcount(r);
+    for (int x = 0; x < (1 << n); ++x) {
+      int v = 0, i = 0;
+      for (int k = 0; k < 4; ++k)
+        if ((r >> k) & 1) v |= ((x >> (n - 1 - i++)) & 1) << k;
+      T.rawmr[r][x] = (uint8_t)v;
+    }
+  }
   for (int band = 0; band < 3; ++band)
     for (int nb = 0; nb < 512; ++nb) {
       int h = ((nb >> 3) & 1) + ((nb >> 5) & 1);

@@ -67,10 +67,13 @@ enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, C_UNI = 18, N_CTX = 19 };
 //              .y = (mps << 16) | (state after an MPS << 8) | state after an LPS
 //   zc[3][512]: zero-coding context for LL/LH, HL, HH neighbourhoods
 //   sc[256]  : (sign context << 1) | xor bit for an 8-bit (sigma, chi) neighbour index
+//   rawmr[r][x]: bypass refinement bits: the n = popcount(r) raw bits x (first decoded in
+//              bit n-1) placed on the rows set in r, lowest row first
 struct T1Tables {
   uint2 mq[96];
   uint8_t zc[3][512];
   uint8_t sc[256];
+  uint8_t rawmr[16][16];
 };
 
 // MQ decoder registers.  Code bytes are read as aligned 32-bit words: `cur` holds the byte
@@ -385,6 +388,19 @@ __device__ __forceinline__ uint32_t magref_column(const BlockSmem &b, uint32_t c
                                                   bool israw, Raw &raw, Mq &mq, const T1Tables &T) {
   const uint32_t refined = *rf;
   uint32_t bits = 0;
+  if (israw) {
+    // bypass: the column's refinement bits are consecutive raw bits, taken together
+    const int n = __popc(rows);
+    uint32_t x = 0;
+    if (raw.ct >= n) {
+      x = (raw.c >> (raw.ct - n)) & ((1u << n) - 1u);
+      raw.ct -= n;
+    } else {
+      for (int i = 0; i < n; ++i) x = (x << 1) | (uint32_t)raw_bit(raw);
+    }
+    if (rows) *rf = (uint8_t)(refined | rows);
+    return rows | ((uint32_t)T.rawmr[rows][x] << 4);
+  }
 #pragma unroll
   for (int i = 0; i < (UNROLLED ? 4 : 1); ++i) {
     uint32_t todo = UNROLLED ? (rows & (1u << i)) : rows;
