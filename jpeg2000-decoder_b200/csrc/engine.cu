@@ -53,7 +53,8 @@ struct T1Layout {
   static constexpr int GAP = MAXW + 3;
   static constexpr int CWN = (STRIPES + 2) * GAP + 2;
   static constexpr int RF_BYTES = ((STRIPES * GAP) + 3) & ~3;
-  static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 8) + 15) & ~15;
+  // context words, refined bits, MQ context slots, then 32 bytes of per-chunk row masks
+  static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 8 + 32) + 15) & ~15;
 };
 
 // Host-side queue classes: code-block size bound.  One class: with 64 registers per thread

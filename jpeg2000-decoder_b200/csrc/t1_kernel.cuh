@@ -493,6 +493,14 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
       uint32_t live = __ballot_sync(0xffffffffu, valid && work);
       uint32_t zero = __ballot_sync(0xffffffffu, valid && word == 0);
       uint32_t dirty = 0;
+      // compact form: the lanes' cleanup / refinement masks go through shared memory (they
+      // depend on a column's own rows only, so they hold while the chunk is decoded; a
+      // register copy would raise the register count above the occupancy budget)
+      uint8_t *lane_masks = reinterpret_cast<uint8_t *>(b.cx + N_CTX);
+      if (!LP && pass != P_SIGPROP) {
+        lane_masks[lane] = (uint8_t)mask;
+        __syncwarp();
+      }
       while (live) {
         const int bit = __ffs(live) - 1;
         if (pass == P_CLEANUP && ((zero >> bit) & 1)) {
@@ -523,7 +531,7 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
           cw = *wp;
         }
         if (pass == P_MAGREF) {
-          const uint32_t rows = LP ? lane_mask : row_mask<0u, V_SIG | V_MU, 0u>(cw);
+          const uint32_t rows = LP ? lane_mask : lane_masks[bit];
           const uint32_t upd = magref_column<UNROLLED>(b, cw, rows, rrow + col, israw, raw, mq, T);
           b.sp.apply_ref(4 * s, col, upd, p);
           continue;
@@ -535,8 +543,8 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
         } else {
           // own-row bits do not change from the left, so the lane's mask holds; a column
           // that was all-zero may have been reached from the left and is not any more
-          const uint32_t todo =
-              (dty && (!LP || lane_word == 0)) ? row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw) : lane_mask;
+          const uint32_t todo = LP ? ((dty && lane_word == 0) ? row_mask<V_SIG | V_CHI | V_PI, 0u, 0u>(cw) : lane_mask)
+                                   : lane_masks[bit];
           upd = cleanup_column<UNROLLED>(b, wp, cw, todo, zc, raw, mq, T);
         }
         *wp = cw;
