@@ -202,19 +202,21 @@ __device__ __forceinline__ void dwt_windows(DwtSmem<REV> *S, int nw, const WinSr
   const int sc_e1 = two ? S[0].scol[2 * (lane + 32)] : 0, sc_o1 = two ? S[0].scol[2 * (lane + 32) + 1] : 0;
   for (int w = 0; w < nw; ++w) {
     const uint32_t tile_s = (uint32_t)__cvta_generic_to_shared(S[w].tile);
-    const WinSrc<REV> in = src[w];
-    for (int rr = warp; rr < 4 * QN; rr += nwarps) {
-      const int qd = rr / QN, r = rr - qd * QN;  // quadrant (LL, HL, LH, HH) and its row
-      const int iy = 2 * r + (qd >> 1), odd = qd & 1;
-      const T *line = qd == 0 ? in.llsrc + (size_t)S[0].srow[iy] * in.stride_ll
-                              : in.quad + (size_t)S[0].srow[iy] * in.stride_q;
-      const uint32_t dst = tile_s + 4u * (iy * DWT_PITCH + odd);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8u * lane), "l"(line + (odd ? sc_o0 : sc_e0))
-                   : "memory");
-      if (two)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8u * (lane + 32)),
-                     "l"(line + (odd ? sc_o1 : sc_e1))
-                     : "memory");
+#pragma unroll
+    for (int qd = 0; qd < 4; ++qd) {  // quadrant LL, HL, LH, HH
+      const T *qbase = qd == 0 ? src[w].llsrc : src[w].quad;
+      const int qstride = qd == 0 ? src[w].stride_ll : src[w].stride_q;
+      const int odd = qd & 1;
+      const T *lo0 = qbase + (odd ? sc_o0 : sc_e0), *lo1 = qbase + (odd ? sc_o1 : sc_e1);
+      const uint32_t d0 = tile_s + 4u * (odd + 2 * lane), d1 = d0 + 4u * 64;
+#pragma unroll 2
+      for (int r = warp; r < QN; r += nwarps) {
+        const int iy = 2 * r + (qd >> 1);
+        const size_t row = (size_t)S[0].srow[iy] * qstride;
+        const uint32_t drow = 4u * iy * DWT_PITCH;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d0 + drow), "l"(lo0 + row));
+        if (two) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d1 + drow), "l"(lo1 + row));
+      }
     }
   }
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -379,7 +381,6 @@ __device__ __forceinline__ void mct_pixel(T y, T u, T w, int dc, int maxv, int *
 template <typename T>
 __device__ __forceinline__ void emit_pixel(const OutGroup &G, uint8_t *out, int yy, int xx, const T *v,
                                            const bool *have) {
-  constexpr bool INT = std::is_integral<T>::value;
   const int pxb = fmt_bytes(G.fmt);
   const int B = G.bitdepth;
   const int outdepth = (pxb == 3 || pxb == 4) ? 8 : 16;
