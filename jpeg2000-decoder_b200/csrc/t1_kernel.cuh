@@ -12,10 +12,14 @@
  * longest blocks first), so CTAs stay resident and uneven blocks balance out.
  *
  * Latency and occupancy measures, none of which changes a decoded bit:
- *   - the kernel is kept small for the instruction cache (many resident warps sit in
- *     different passes at once): each pass visits the four rows of a stripe column in a
- *     loop rather than unrolled, inlines each of its decisions once, and bypass (raw) and
- *     MQ decisions share the pass code; one renormalisation site per MQ decision;
+ *   - two kernel forms: the compact one (long queues, throughput) is kept small for the
+ *     instruction cache (many resident warps sit in different passes at once): each pass
+ *     walks the rows of a stripe column as a bit mask, inlines each of its decisions once,
+ *     and bypass (raw) and MQ decisions share the pass code; the unrolled one (batches that
+ *     fit about two waves, latency) unrolls the rows and hands the lanes' chunk words and
+ *     masks to the serial loop;
+ *   - per 32-column chunk the lanes compute each column's row mask and only columns with
+ *     work join the serial loop;
  *   - each MQ context slot holds its probability-table entry (Qe, MPS, both successor
  *     states), so a symbol needs one shared-memory load before its decision;
  *   - code bytes are read as aligned 32-bit words with the next word requested early, so
@@ -25,11 +29,13 @@
  *     consumed in one step: A -= k*Qe, C -= k*Qe;
  *   - samples live in the block's own region of the output buffer, not in shared memory:
  *     they are only written while decoding (significance sets sign + 1.5 * 2^p, a
- *     refinement flips bit p and sets the new midpoint bit), so one lane issues a
- *     fire-and-forget atomic XOR per update, and the "first refinement?" context test of
- *     the reference ((|v| >> p) < 4, true exactly on a sample's first refinement) reads a
- *     per-sample "refined" bit kept in shared memory.  A 64x64 block then needs 5.9 KB of
- *     shared memory instead of 13-21 KB, so more blocks are resident per SM.
+ *     refinement flips bit p and sets the new midpoint bit), so a stripe column's updates
+ *     go out at its end as fire-and-forget atomic XORs from lanes 0..3 in one instruction,
+ *     and the "first refinement?" context test of the reference ((|v| >> p) < 4, true
+ *     exactly on a sample's first refinement) reads a per-sample "refined" bit kept in
+ *     shared memory.  A 64x64 block then needs 6 KB of shared memory instead of 13-21 KB,
+ *     so more blocks are resident per SM;
+ *   - bypass refinement bits of a column are taken together and scattered to their rows.
  *
  * Semantics follow the reference block decoder exactly (decoder/codec/src/
  * bmi_block_decoder.cpp:10-853, bmi_mq_decoder.h/.cpp, bmi_t1_macro.h): same context-word
