@@ -44,35 +44,42 @@ struct Reader {
   }
 };
 
-// packet-header bit reader with 0xFF bit stuffing (T.800 B.10.1)
+// packet-header bit reader with 0xFF bit stuffing (T.800 B.10.1): after a 0xFF byte the
+// next byte carries 7 bits (its most significant bit is a stuffed 0).  Bits are buffered in
+// a 64-bit accumulator a byte at a time, so multi-bit fields are read in one step.
 struct BitReader {
   const uint8_t *p, *end;
-  uint32_t c = 0;
-  int ct = 0;
+  uint32_t c = 0;     // the last byte read (0xFF decides the next byte's width)
+  uint64_t acc = 0;   // unread bits, right-aligned
+  int nacc = 0;       // number of unread bits
   bool overrun = false;
-  int bit() {
-    if (ct == 0) {
-      uint32_t prev = c;
-      if (p >= end) {
-        overrun = true;
-        c = 0;
-      } else {
-        c = *p++;
-      }
-      ct = (prev == 0xFF) ? 7 : 8;
+  void refill() {
+    const uint32_t prev = c;
+    if (p >= end) {
+      overrun = true;
+      c = 0;
+    } else {
+      c = *p++;
     }
-    --ct;
-    return (c >> ct) & 1;
+    const int nb = (prev == 0xFF) ? 7 : 8;
+    acc = (acc << nb) | (c & ((1u << nb) - 1u));
+    nacc += nb;
+  }
+  int bit() {
+    if (nacc == 0) refill();
+    --nacc;
+    return (int)((acc >> nacc) & 1);
   }
   uint32_t bits(int n) {
-    uint32_t v = 0;
-    for (int i = 0; i < n; ++i) v = (v << 1) | (uint32_t)bit();
-    return v;
+    while (nacc < n) refill();
+    nacc -= n;
+    return (uint32_t)((acc >> nacc) & ((n >= 32) ? 0xFFFFFFFFull : ((1ull << n) - 1)));
   }
   // end of header: byte aligned, a byte after 0xFF is consumed as well
   void align() {
     if (c == 0xFF && p < end) ++p;  // a header ending on 0xFF is followed by a stuffed byte
-    ct = 0;
+    nacc = 0;
+    acc = 0;
     c = 0;
   }
 };
@@ -410,6 +417,7 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
 }
 
 int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImagePlan &P) {
+  P.bytes.reserve(len);  // the coded bytes of every block are a subset of the codestream
   P = ImagePlan();
   int st = parse_header(data, len, P.hdr);
   if (st != PARSE_OK) return st;
@@ -571,8 +579,11 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
                   cb.y0 = gy0 - B.y0;
                   cb.w = gx1 - gx0;
                   cb.h = gy1 - gy0;
+                  // one piece per contributing layer, usually one segment per layer
+                  cb.pieces.reserve(std::min(H.layers, 16));
+                  cb.seglen.reserve(std::min(H.layers, 16));
                   B.prec_cbs[p].push_back((int)B.cbs.size());
-                  B.cbs.push_back(cb);
+                  B.cbs.push_back(std::move(cb));
                 }
             }
         }
@@ -594,6 +605,16 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     };
     next_part();
     bool stream_end = false;
+    // one packet's code-block contributions; reused across packets (no allocation per
+    // contribution): segment lengths live in one flat buffer
+    struct Contrib {
+      CbState *cb;
+      uint32_t lens_at, nlens;
+      int newpasses;
+      int first_seg_new;  // whether the first piece opens a new segment
+    };
+    std::vector<Contrib> contribs;
+    std::vector<uint32_t> lens;
     auto read_packet = [&](int l, int r, int c, int p) -> int {
       TCState &TC = tcs[c];
       if (r > TC.levels) return PARSE_OK;
@@ -607,13 +628,8 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       }
       if (H.sop && end - cur >= 6 && cur[0] == 0xFF && cur[1] == 0x91) cur += 6;
       BitReader br{cur, end};
-      struct Contrib {
-        CbState *cb;
-        std::vector<uint32_t> lens;
-        int newpasses;
-        int first_seg_new;  // whether the first piece opens a new segment
-      };
-      std::vector<Contrib> contribs;
+      contribs.clear();
+      lens.clear();
       if (br.bit()) {
         for (auto &B : R.bands) {
           if (B.prec_cbs.empty() || B.prec_cbs[p].empty()) continue;
@@ -649,19 +665,20 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             while (br.bit()) {
               if (++cb.lblock > 32 || br.overrun) return PARSE_ERR_PACKET;
             }
-            Contrib ct{&cb, {}, n, 0};
+            Contrib ct{&cb, (uint32_t)lens.size(), 0, n, 0};
             int s = cb.passes;
             while (s < cb.passes + n) {
               int e = s + 1;
               while (e < cb.passes + n && !seg_starts(H.cbstyle[c], e)) ++e;
               int nb = cb.lblock + floor_log2((uint32_t)(e - s));
               if (nb > 32) return PARSE_ERR_PACKET;
-              ct.lens.push_back(br.bits(nb));
+              lens.push_back(br.bits(nb));
               if (s == cb.passes) ct.first_seg_new = seg_starts(H.cbstyle[c], s);
               s = e;
             }
             if (br.overrun) return PARSE_ERR_PACKET;
-            contribs.push_back(std::move(ct));
+            ct.nlens = (uint32_t)lens.size() - ct.lens_at;
+            contribs.push_back(ct);
             (void)gw;
           }
         }
@@ -674,8 +691,8 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       const bool keep = l < maxlayers;
       for (auto &ct : contribs) {
         CbState &cb = *ct.cb;
-        for (size_t i = 0; i < ct.lens.size(); ++i) {
-          uint32_t L = ct.lens[i];
+        for (uint32_t i = 0; i < ct.nlens; ++i) {
+          uint32_t L = lens[ct.lens_at + i];
           if ((size_t)(end - cur) < L) {
             // truncated packet body: keep what is there, stop the tile
             L = (uint32_t)(end - cur);
