@@ -117,6 +117,12 @@ int j2k_gpu_image_status(const j2k_gpu_ctx *ctx, int slot, int *bad_blocks);
 /* Packed output of a slot (device pointer valid until the next batch_begin). */
 int j2k_gpu_output_device(const j2k_gpu_ctx *ctx, int slot, const void **dptr, size_t *bytes);
 int j2k_gpu_output_copy(j2k_gpu_ctx *ctx, int slot, void *host_dst, size_t bytes);
+/* Enqueue the copy of a slot's packed output into `host_dst` behind the batch's decode,
+ * between batch_launch (or batch_run) and batch_sync.  The copy overlaps whatever the host
+ * does next; batch_sync returns only once every copy enqueued this way has landed, so
+ * `host_dst` (pinned memory, for the copy to be asynchronous) must stay valid until then.
+ * The counterpart of a GetResult into the output queue without a host wait per picture. */
+int j2k_gpu_output_copy_async(j2k_gpu_ctx *ctx, int slot, void *host_dst, size_t bytes);
 /* Decoded (un-shifted) component samples of a slot as int32 (5/3) or float32 (9/7),
  * row-major over the output size: the reference's GetDecodedComponentInt / Float
  * (decoder/core/src/decoderconcrete.cpp:531-584).  J2K_ERR_STATE for an image added with a

@@ -246,6 +246,7 @@ struct j2k_gpu_ctx {
   uint16_t *h_status = nullptr;  // pinned
   size_t h_status_cap = 0;
   bool launched = false, synced = false, staged = false;
+  bool copies_pending = false;  // output copies enqueued behind the decode (ev[5] follows them)
   // staged batch (device-resident inputs) for batch_run
   struct Staged {
     size_t nq[NQ] = {0}, n_cblks = 0, n_otasks = 0;
@@ -255,7 +256,7 @@ struct j2k_gpu_ctx {
     int maxL = 0;
     std::vector<uint32_t> dtask_off;
   } sg;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[6] = {};  // h2d start, h2d end, Tier-1 end, DWT end, decode end, output copies end
   float t_t1 = 0, t_dwt = 0, t_h2d = 0, t_total = 0;
   int launches = 0;
   j2k_gpu_tuning tuning{8, 64, 0, 0, 2};
@@ -415,7 +416,7 @@ extern "C" int j2k_gpu_batch_begin(j2k_gpu_ctx *c) {
   if (!c) return J2K_ERR_ARG;
   if (c->launched && !c->synced) return J2K_ERR_STATE;
   c->imgs.clear();
-  c->launched = c->synced = c->staged = false;
+  c->launched = c->synced = c->staged = c->copies_pending = false;
   return J2K_OK;
 }
 
@@ -977,6 +978,7 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   }
   c->launched = true;
   c->synced = false;
+  c->copies_pending = false;
   return J2K_OK;
 }
 
@@ -992,8 +994,10 @@ extern "C" int j2k_gpu_batch_sync(j2k_gpu_ctx *c, int timeout_ms) {
   if (c->synced) return J2K_OK;
   cudaSetDevice(c->device);
   auto t0 = std::chrono::steady_clock::now();
+  // ev[5] is recorded after ev[4] on the same stream: it covers the decode and the copies
+  cudaEvent_t done = c->copies_pending ? c->ev[5] : c->ev[4];
   for (;;) {
-    cudaError_t e = cudaEventQuery(c->ev[4]);
+    cudaError_t e = cudaEventQuery(done);
     if (e == cudaSuccess) break;
     if (e != cudaErrorNotReady) return J2K_ERR_CUDA;
     if (timeout_ms == 0) return J2K_ERR_TIMEOUT;  // poll once
@@ -1016,6 +1020,7 @@ extern "C" int j2k_gpu_batch_sync(j2k_gpu_ctx *c, int timeout_ms) {
     im.status = bad ? J2K_ERR_DECODE : J2K_OK;
   }
   c->synced = true;
+  c->copies_pending = false;
   return J2K_OK;
 }
 
@@ -1043,6 +1048,19 @@ extern "C" int j2k_gpu_output_copy(j2k_gpu_ctx *c, int slot, void *dst, size_t b
   CK(cudaMemcpyAsync(dst, (const uint8_t *)c->d_out.p + im.out_base, im.out_bytes, cudaMemcpyDeviceToHost,
                      c->user_stream));
   CK(cudaStreamSynchronize(c->user_stream));
+  return J2K_OK;
+}
+
+extern "C" int j2k_gpu_output_copy_async(j2k_gpu_ctx *c, int slot, void *dst, size_t bytes) {
+  if (!c || slot < 0 || slot >= (int)c->imgs.size() || !dst) return J2K_ERR_ARG;
+  if (!c->launched || c->synced) return J2K_ERR_STATE;
+  const BatchImage &im = c->imgs[slot];
+  if (bytes < im.out_bytes) return J2K_ERR_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaMemcpyAsync(dst, (const uint8_t *)c->d_out.p + im.out_base, im.out_bytes, cudaMemcpyDeviceToHost,
+                     c->user_stream));
+  CK(cudaEventRecord(c->ev[5], c->user_stream));
+  c->copies_pending = true;
   return J2K_OK;
 }
 

@@ -35,6 +35,7 @@ J2K_ERR_NODEVICE = -9
 J2K_ERR_DECODE = -7
 J2K_ERR_TIMEOUT = -6
 J2K_ERR_NOMEM = -5
+J2K_ERR_STATE = -8
 
 
 class J2kError(RuntimeError):
@@ -102,7 +103,8 @@ EXPORTS = [
     "j2k_plan_bytes", "j2k_plan_tilecomps", "j2k_output_bytes", "j2k_status_string",
     "j2k_gpu_ctx_create", "j2k_gpu_ctx_destroy", "j2k_gpu_mem_usage", "j2k_gpu_batch_begin",
     "j2k_gpu_batch_add", "j2k_gpu_batch_footprint", "j2k_gpu_batch_launch", "j2k_gpu_batch_stage", "j2k_gpu_batch_run", "j2k_gpu_batch_sync",
-    "j2k_gpu_image_status", "j2k_gpu_output_device", "j2k_gpu_output_copy", "j2k_gpu_component_copy",
+    "j2k_gpu_image_status", "j2k_gpu_output_device", "j2k_gpu_output_copy", "j2k_gpu_output_copy_async",
+    "j2k_gpu_component_copy",
     "j2k_gpu_coefficients_copy", "j2k_gpu_last_timing", "j2k_gpu_last_launches", "j2k_gpu_set_tuning",
     "j2k_gpu_get_tuning", "j2k_gpu_autotune", "j2k_gpu_decode", "j2k_gpu_tile_idwt_noalloc",
     "j2k_server_create", "j2k_server_destroy", "j2k_server_submit", "j2k_server_wait", "j2k_server_result",
@@ -147,6 +149,7 @@ def lib():
         L.j2k_gpu_image_status.argtypes = [vp, i, ctypes.POINTER(i)]
         L.j2k_gpu_output_device.argtypes = [vp, i, ctypes.POINTER(vp), ctypes.POINTER(sz)]
         L.j2k_gpu_output_copy.argtypes = [vp, i, vp, sz]
+        L.j2k_gpu_output_copy_async.argtypes = [vp, i, vp, sz]
         L.j2k_gpu_component_copy.argtypes = [vp, i, i, vp, sz]
         L.j2k_gpu_coefficients_copy.argtypes = [vp, i, i, vp, sz]
         f = ctypes.POINTER(ctypes.c_float)
@@ -353,6 +356,11 @@ class GpuContext:
         out = np.empty(n, np.uint8)
         self._ck(lib().j2k_gpu_output_copy(self.h, slot, out.ctypes.data_as(ctypes.c_void_p), n), "output_copy")
         return out
+
+    def output_async(self, slot, ptr, nbytes):
+        """Enqueue the copy of a slot's output to host address `ptr` (pinned) behind the
+        decode; the next sync() covers it.  The buffer must outlive that sync."""
+        self._ck(lib().j2k_gpu_output_copy_async(self.h, slot, ctypes.c_void_p(ptr), nbytes), "output_copy_async")
 
     def component(self, slot, comp):
         plan, _ = self.plans[slot]

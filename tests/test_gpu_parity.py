@@ -150,6 +150,39 @@ def test_batch_alone_equals_mixed(gpu_ctx):
         assert np.array_equal(gpu_ctx.output(s), want)
 
 
+def test_async_output_copies_land_by_sync(gpu_ctx):
+    """Output copies enqueued behind the decode (pinned destinations) hold every picture
+    once batch_sync returns; outside launch..sync the call is refused with J2K_ERR_STATE."""
+    import torch
+    from jpeg2000_decoder_b200 import native, synth
+    streams = [synth.c5_request(s)[0] for s in range(4)] + [_read("rgb256_97_1bpp.j2k")]
+    plans = [native.Plan(cs) for cs in streams]
+    fmts = [native.FMT_48BITS_RGB if p.info.bitdepth > 8 else native.FMT_24BITS_RGB for p in plans]
+    gpu_ctx.begin()
+    slots = [gpu_ctx.add(p, f) for p, f in zip(plans, fmts)]
+    dst = [torch.zeros(p.output_bytes(f), dtype=torch.uint8).pin_memory() for p, f in zip(plans, fmts)]
+    lib = native.lib()
+    assert lib.j2k_gpu_output_copy_async(gpu_ctx.h, 0, ctypes.c_void_p(dst[0].data_ptr()),
+                                         dst[0].numel()) == native.J2K_ERR_STATE
+    gpu_ctx.launch()
+    for s, d in zip(slots, dst):
+        gpu_ctx.output_async(s, d.data_ptr(), d.numel())
+    assert gpu_ctx.sync() == 0
+    assert lib.j2k_gpu_output_copy_async(gpu_ctx.h, 0, ctypes.c_void_p(dst[0].data_ptr()),
+                                         dst[0].numel()) == native.J2K_ERR_STATE
+    for s, d in zip(slots, dst):
+        assert gpu_ctx.status(s)[0] == 0
+        assert np.array_equal(d.numpy(), gpu_ctx.output(s))
+    # a second batch on the same context: copies of the new batch only
+    gpu_ctx.begin()
+    s0 = gpu_ctx.add(plans[-1], fmts[-1])
+    d0 = torch.zeros(plans[-1].output_bytes(fmts[-1]), dtype=torch.uint8).pin_memory()
+    gpu_ctx.launch()
+    gpu_ctx.output_async(s0, d0.data_ptr(), d0.numel())
+    assert gpu_ctx.sync() == 0
+    assert np.array_equal(d0.numpy(), gpu_ctx.output(s0))
+
+
 def test_components_and_reduced_resolution(gpu_ctx):
     from jpeg2000_decoder_b200 import native
     cs = _read("rgb300x200_97_tiles_3layers.j2k")
