@@ -10,11 +10,15 @@
  *
  * Differences from the reference front end, by design: codeword segments are tracked per
  * code-block (the reference treats the whole pass list as one segment,
- * bmi_block_decoder.cpp:735-768), so BYPASS/RESET/TERMALL streams are planned correctly.
+ * bmi_block_decoder.cpp:735-768), so BYPASS/RESET/TERMALL streams are planned correctly;
+ * the 9/7 magnitude bit count is exponent + guard bits - 1 (T.800 E.1.1.1) where the
+ * reference adds the guard bits to the raw exponent/mantissa word (dec_jp2.cpp:177-178),
+ * which agrees only for one guard bit.
  */
 #include "codestream.h"
 
 #include <algorithm>
+#include <memory>
 #include <cstring>
 
 namespace j2k {
@@ -243,6 +247,151 @@ static size_t find_codestream(const uint8_t *d, size_t len) {
   return 0;
 }
 
+namespace {
+
+// SPcod / SPcoc of one component (T.800 Table A.15): levels, code-block size and style,
+// transform, precinct sizes
+int read_spcod(Reader &s, StreamHeader &H, int c, bool user_precincts) {
+  const int lev = (int)s.u8();
+  const int xcb = (int)s.u8() + 2, ycb = (int)s.u8() + 2;
+  const int style = (int)s.u8();
+  const int rev = s.u8() == 1;
+  if (lev > J2K_MAX_LEVELS) return PARSE_ERR_UNSUPPORTED;
+  H.levels[c] = lev;
+  H.cbw_exp[c] = xcb;
+  H.cbh_exp[c] = ycb;
+  H.cbstyle[c] = style;
+  H.reversible[c] = rev;
+  for (int i = 0; i <= lev; ++i) {
+    if (user_precincts) {
+      unsigned pp = s.u8();
+      H.ppx[c][i] = pp & 0xF;
+      H.ppy[c][i] = pp >> 4;
+      if (i > 0 && (H.ppx[c][i] == 0 || H.ppy[c][i] == 0)) return PARSE_ERR_INVALID;
+    } else {
+      H.ppx[c][i] = H.ppy[c][i] = 15;
+    }
+  }
+  return s.ok ? PARSE_OK : PARSE_ERR_TRUNCATED;
+}
+
+// COD (A.6.1): the image- or tile-wide SGcod, and SPcod for every component that no COC of
+// equal or higher precedence has set (`comp_set`)
+int read_cod(Reader s, StreamHeader &H, const bool *comp_set) {
+  const unsigned scod = s.u8();
+  H.progression = (int)s.u8();
+  H.layers = (int)s.u16();
+  H.mct = (int)s.u8();
+  H.sop = (scod >> 1) & 1;
+  H.eph = (scod >> 2) & 1;
+  if (!s.ok) return PARSE_ERR_TRUNCATED;
+  if (H.progression > 4) return PARSE_ERR_INVALID;
+  for (int c = 0; c < J2K_MAX_COMPONENTS; ++c) {
+    if (comp_set[c]) continue;
+    Reader t = s;
+    const int rc = read_spcod(t, H, c, scod & 1);
+    if (rc != PARSE_OK) return rc;
+  }
+  return PARSE_OK;
+}
+
+// COC (A.6.2)
+int read_coc(Reader s, StreamHeader &H, bool *comp_set) {
+  const int c = H.ncomp < 257 ? (int)s.u8() : (int)s.u16();
+  if (c >= H.ncomp) return PARSE_ERR_INVALID;
+  const unsigned scoc = s.u8();
+  const int rc = read_spcod(s, H, c, scoc & 1);
+  comp_set[c] = true;
+  return rc;
+}
+
+// QCD / QCC (A.6.4, A.6.5); a QCD leaves the components that a QCC of equal or higher
+// precedence has set (`comp_set`)
+int read_qcx(Reader s, bool qcc, StreamHeader &H, bool *comp_set) {
+  int c0 = 0, c1 = J2K_MAX_COMPONENTS;
+  if (qcc) {
+    c0 = H.ncomp < 257 ? (int)s.u8() : (int)s.u16();
+    if (c0 >= H.ncomp) return PARSE_ERR_INVALID;
+    c1 = c0 + 1;
+  }
+  const unsigned sq = s.u8();
+  const int style = sq & 0x1F, guard = (int)(sq >> 5);
+  std::vector<uint16_t> st;
+  while (s.left() > 0) {
+    if (style == 0) st.push_back((uint16_t)(s.u8() >> 3));
+    else st.push_back((uint16_t)s.u16());
+  }
+  if (!s.ok) return PARSE_ERR_TRUNCATED;
+  if (style > 2 || (style == 1 && st.size() != 1)) return PARSE_ERR_INVALID;
+  if (st.empty() || st.size() > 3 * J2K_MAX_LEVELS + 1) return PARSE_ERR_INVALID;
+  for (int c = c0; c < c1; ++c) {
+    if (!qcc && comp_set[c]) continue;
+    H.qstyle[c] = style;
+    H.guard[c] = guard;
+    for (size_t i = 0; i < 3 * J2K_MAX_LEVELS + 1; ++i) H.steps[c][i] = i < st.size() ? st[i] : 0;
+    if (qcc) comp_set[c] = true;
+  }
+  return PARSE_OK;
+}
+
+// RGN (A.6.3): only the shift is kept (a non-zero shift is refused later)
+int read_rgn(Reader s, StreamHeader &H) {
+  const int c = H.ncomp < 257 ? (int)s.u8() : (int)s.u16();
+  s.u8();
+  const int shift = (int)s.u8();
+  if (!s.ok) return PARSE_ERR_TRUNCATED;
+  if (c < J2K_MAX_COMPONENTS) H.roi_shift[c] = shift;
+  return PARSE_OK;
+}
+
+// POC (A.6.6): progression volumes appended to `out`; CEpoc 0 stands for 256 (8-bit form)
+int read_poc(Reader s, int ncomp, std::vector<PocEntry> &out) {
+  const bool wide = ncomp >= 257;
+  const size_t entry = wide ? 9 : 7;
+  if (s.left() == 0 || s.left() % entry) return PARSE_ERR_INVALID;
+  while (s.left() >= entry) {
+    PocEntry e;
+    e.rs = (int)s.u8();
+    e.cs = wide ? (int)s.u16() : (int)s.u8();
+    e.lye = (int)s.u16();
+    e.re = (int)s.u8();
+    e.ce = wide ? (int)s.u16() : (int)s.u8();
+    if (!wide && e.ce == 0) e.ce = 256;
+    e.prog = (int)s.u8();
+    if (e.prog > 4) return PARSE_ERR_INVALID;
+    out.push_back(e);
+  }
+  return PARSE_OK;
+}
+
+// checks of the coding parameters against what the plan and the device path support, and
+// the expansion of scalar-derived quantisation (T.800 E.1.1.1); `main` is the main header
+// when H is a tile's parameters
+int finish_coding(StreamHeader &H, const StreamHeader *main) {
+  if (H.layers < 1) return PARSE_ERR_INVALID;
+  for (int c = 0; c < H.ncomp; ++c) {
+    if (H.cbw_exp[c] > 10 || H.cbh_exp[c] > 10 || H.cbw_exp[c] + H.cbh_exp[c] > 12) return PARSE_ERR_INVALID;
+    if (H.cbw_exp[c] > 6 || H.cbh_exp[c] > 6) return PARSE_ERR_UNSUPPORTED;  // device kernels: <= 64
+    if (H.cbstyle[c] & J2K_CB_CAUSAL) return PARSE_ERR_UNSUPPORTED;
+    if (H.roi_shift[c]) return PARSE_ERR_UNSUPPORTED;
+    // the device runs one wavelet and one inverse MCT per image
+    if (H.reversible[c] != H.reversible[0]) return PARSE_ERR_UNSUPPORTED;
+    if (H.qstyle[c] == 1) {  // scalar derived: expand to the expounded form
+      uint16_t b = H.steps[c][0];
+      int eps0 = b >> 11, mu0 = b & 0x7FF;
+      for (int i = 1; i <= 3 * H.levels[c]; ++i) {
+        int nb = H.levels[c] - (i - 1) / 3;
+        int eps = eps0 - H.levels[c] + nb;
+        H.steps[c][i] = (uint16_t)(((eps < 0 ? 0 : eps) << 11) | mu0);
+      }
+    }
+  }
+  if (main && (H.reversible[0] != main->reversible[0] || H.mct != main->mct)) return PARSE_ERR_UNSUPPORTED;
+  return PARSE_OK;
+}
+
+}  // namespace
+
 int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   H = StreamHeader();
   size_t off = find_codestream(data, len);
@@ -252,6 +401,7 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   if (r.u16() != 0xFF4F) return PARSE_ERR_MARKER;
   bool have_siz = false, have_cod = false, have_qcd = false;
   bool coc_set[J2K_MAX_COMPONENTS] = {false}, qcc_set[J2K_MAX_COMPONENTS] = {false};
+  std::vector<std::pair<int, std::pair<const uint8_t *, size_t>>> ppm;  // (Zppm, payload)
   for (;;) {
     if (r.left() < 4) return PARSE_ERR_TRUNCATED;
     unsigned m = r.u16();
@@ -264,6 +414,8 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
     if (lseg < 2 || lseg - 2 > r.left()) return PARSE_ERR_TRUNCATED;
     Reader s{r.p, r.p + (lseg - 2)};
     r.p += lseg - 2;
+    int rc = PARSE_OK;
+    if (m != 0xFF51 && m != 0xFF64 && !have_siz) return PARSE_ERR_MARKER;  // SIZ comes first
     switch (m) {
       case 0xFF51: {  // SIZ
         s.u16();
@@ -288,104 +440,32 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
         have_siz = true;
         break;
       }
-      case 0xFF52: {  // COD
-        unsigned scod = s.u8();
-        H.progression = (int)s.u8();
-        H.layers = (int)s.u16();
-        H.mct = (int)s.u8();
-        int lev = (int)s.u8();
-        int xcb = (int)s.u8() + 2, ycb = (int)s.u8() + 2;
-        int style = (int)s.u8();
-        int rev = s.u8() == 1;
-        H.sop = (scod >> 1) & 1;
-        H.eph = (scod >> 2) & 1;
-        if (lev > J2K_MAX_LEVELS) return PARSE_ERR_UNSUPPORTED;
-        for (int c = 0; c < J2K_MAX_COMPONENTS; ++c) {
-          if (coc_set[c]) continue;
-          H.levels[c] = lev;
-          H.cbw_exp[c] = xcb;
-          H.cbh_exp[c] = ycb;
-          H.cbstyle[c] = style;
-          H.reversible[c] = rev;
-          for (int i = 0; i <= lev; ++i) {
-            if (scod & 1) {
-              unsigned pp = s.u8();
-              H.ppx[c][i] = pp & 0xF;
-              H.ppy[c][i] = pp >> 4;
-            } else {
-              H.ppx[c][i] = H.ppy[c][i] = 15;
-            }
-          }
-          if (scod & 1) s.p -= (lev + 1);  // re-read precinct sizes for the next component
-        }
-        if (!s.ok) return PARSE_ERR_TRUNCATED;
+      case 0xFF52:  // COD
+        rc = read_cod(s, H, coc_set);
         have_cod = true;
         break;
-      }
-      case 0xFF53: {  // COC
-        if (!have_siz) return PARSE_ERR_MARKER;
-        int c = H.ncomp < 257 ? (int)s.u8() : (int)s.u16();
-        if (c >= H.ncomp) return PARSE_ERR_INVALID;
-        unsigned scoc = s.u8();
-        int lev = (int)s.u8();
-        if (lev > J2K_MAX_LEVELS) return PARSE_ERR_UNSUPPORTED;
-        H.levels[c] = lev;
-        H.cbw_exp[c] = (int)s.u8() + 2;
-        H.cbh_exp[c] = (int)s.u8() + 2;
-        H.cbstyle[c] = (int)s.u8();
-        H.reversible[c] = s.u8() == 1;
-        for (int i = 0; i <= lev; ++i) {
-          if (scoc & 1) {
-            unsigned pp = s.u8();
-            H.ppx[c][i] = pp & 0xF;
-            H.ppy[c][i] = pp >> 4;
-          } else {
-            H.ppx[c][i] = H.ppy[c][i] = 15;
-          }
-        }
-        coc_set[c] = true;
+      case 0xFF53:  // COC
+        rc = read_coc(s, H, coc_set);
         break;
-      }
-      case 0xFF5C:    // QCD
-      case 0xFF5D: {  // QCC
-        int c0 = 0, c1 = J2K_MAX_COMPONENTS;
-        if (m == 0xFF5D) {
-          if (!have_siz) return PARSE_ERR_MARKER;
-          c0 = H.ncomp < 257 ? (int)s.u8() : (int)s.u16();
-          if (c0 >= H.ncomp) return PARSE_ERR_INVALID;
-          c1 = c0 + 1;
-        }
-        unsigned sq = s.u8();
-        int style = sq & 0x1F, guard = (int)(sq >> 5);
-        std::vector<uint16_t> st;
-        while (s.left() > 0) {
-          if (style == 0) st.push_back((uint16_t)(s.u8() >> 3));
-          else st.push_back((uint16_t)s.u16());
-        }
-        if (style == 1 && st.size() != 1) return PARSE_ERR_INVALID;
-        if (st.empty() || st.size() > 3 * J2K_MAX_LEVELS + 1) return PARSE_ERR_INVALID;
-        for (int c = c0; c < c1; ++c) {
-          if (m == 0xFF5C && qcc_set[c]) continue;
-          H.qstyle[c] = style;
-          H.guard[c] = guard;
-          for (size_t i = 0; i < 3 * J2K_MAX_LEVELS + 1; ++i) H.steps[c][i] = i < st.size() ? st[i] : 0;
-          if (m == 0xFF5D) qcc_set[c] = true;
-        }
-        have_qcd = true;
+      case 0xFF5C:  // QCD
+      case 0xFF5D:  // QCC
+        rc = read_qcx(s, m == 0xFF5D, H, qcc_set);
+        if (m == 0xFF5C) have_qcd = true;
         break;
-      }
-      case 0xFF5E: {  // RGN
-        int c = H.ncomp < 257 ? (int)s.u8() : (int)s.u16();
-        s.u8();
-        if (c < J2K_MAX_COMPONENTS) H.roi_shift[c] = (int)s.u8();
+      case 0xFF5E:  // RGN
+        rc = read_rgn(s, H);
         break;
-      }
       case 0xFF5F:  // POC
-      case 0xFF60:  // PPM
-        return PARSE_ERR_UNSUPPORTED;
+        rc = read_poc(s, H.ncomp, H.poc);
+        break;
+      case 0xFF60:  // PPM: packed packet headers of every tile-part, in Zppm order
+        if (s.left() < 1) return PARSE_ERR_TRUNCATED;
+        ppm.push_back({(int)s.p[0], {s.p + 1, s.left() - 1}});
+        break;
       default:  // COM, TLM, PLM, CRG and others are skipped
         break;
     }
+    if (rc != PARSE_OK) return rc;
   }
   if (!have_siz || !have_cod || !have_qcd) return PARSE_ERR_MARKER;
   if (H.width <= H.x0 || H.height <= H.y0 || H.tile_w <= 0 || H.tile_h <= 0) return PARSE_ERR_INVALID;
@@ -393,46 +473,37 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   for (int c = 0; c < H.ncomp; ++c) {
     if (H.sub_x[c] != 1 || H.sub_y[c] != 1) return PARSE_ERR_UNSUPPORTED;
     if (H.depth[c] > 16 || H.depth[c] != H.depth[0]) return PARSE_ERR_UNSUPPORTED;
-    if (H.cbw_exp[c] > 10 || H.cbh_exp[c] > 10 || H.cbw_exp[c] + H.cbh_exp[c] > 12) return PARSE_ERR_INVALID;
-    if (H.cbw_exp[c] > 6 || H.cbh_exp[c] > 6) return PARSE_ERR_UNSUPPORTED;  // device kernels: <= 64
-    if (H.cbstyle[c] & J2K_CB_CAUSAL) return PARSE_ERR_UNSUPPORTED;
-    if (H.roi_shift[c]) return PARSE_ERR_UNSUPPORTED;
-    if (H.qstyle[c] == 1) {  // scalar derived: expand to the expounded form (T.800 E.1.1.1)
-      uint16_t b = H.steps[c][0];
-      int eps0 = b >> 11, mu0 = b & 0x7FF;
-      for (int i = 1; i <= 3 * H.levels[c]; ++i) {
-        int nb = H.levels[c] - (i - 1) / 3;
-        int eps = eps0 - H.levels[c] + nb;
-        H.steps[c][i] = (uint16_t)(((eps < 0 ? 0 : eps) << 11) | mu0);
-      }
-    }
-    if (H.reversible[c] != (H.qstyle[c] == 0)) {
-      // reversible transform with quantisation (or the reverse) is legal but not in the
-      // reference's decode path; accept and follow the transform flag
-    }
   }
-  if (H.layers < 1) return PARSE_ERR_INVALID;
+  int rc = finish_coding(H, nullptr);
+  if (rc != PARSE_OK) return rc;
+  if (!ppm.empty()) {
+    std::stable_sort(ppm.begin(), ppm.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+    for (auto &seg : ppm) H.ppm.insert(H.ppm.end(), seg.second.first, seg.second.first + seg.second.second);
+    H.has_ppm = true;
+  }
   H.header_len = (size_t)(r.p - data);
   return PARSE_OK;
 }
 
 int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImagePlan &P) {
-  P.bytes.reserve(len);  // the coded bytes of every block are a subset of the codestream
   P = ImagePlan();
+  P.bytes.reserve(len);  // the coded bytes of every block are a subset of the codestream
   int st = parse_header(data, len, P.hdr);
   if (st != PARSE_OK) return st;
   const StreamHeader &H = P.hdr;
   const int ntx = H.ntx(), nty = H.nty(), ntiles = ntx * nty;
-  const int maxlayers = opt.max_layers > 0 ? std::min(opt.max_layers, H.layers) : H.layers;
-  int discard = opt.discard_levels;
-  for (int c = 0; c < H.ncomp; ++c) discard = std::min(discard, H.levels[c]);
-  if (discard < 0) discard = 0;
-  P.discard = discard;
 
-  // ---- gather tile-part bodies per tile (T.800 A.4)
+  // ---- gather tile-parts per tile (T.800 A.4): bodies, the tile's own coding parameters
+  // (COD/COC/QCD/QCC/RGN of its first tile-part), its POC volumes and its packed packet
+  // headers (PPT segments, or this tile-part's share of the main header's PPM data)
   std::vector<std::vector<std::pair<const uint8_t *, size_t>>> tparts(ntiles);
+  std::vector<std::unique_ptr<StreamHeader>> thdr(ntiles);
+  std::vector<std::vector<uint8_t>> packed(ntiles);
+  std::vector<char> has_packed(ntiles, H.has_ppm ? 1 : 0);
   {
     Reader r{data + H.header_len, data + len};
+    size_t ppm_pos = 0;
+    std::vector<bool> tile_seen(ntiles, false), tile_poc(ntiles, false);
     for (;;) {
       if (r.left() < 2) return PARSE_ERR_TRUNCATED;
       unsigned m = r.u16();
@@ -442,20 +513,60 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       unsigned lsot = r.u16();
       unsigned isot = r.u16();
       uint32_t psot = r.u32();
-      r.u8();
-      r.u8();
+      r.u8();  // TPsot
+      r.u8();  // TNsot
       if (!r.ok || lsot != 10) return PARSE_ERR_TRUNCATED;
       if ((int)isot >= ntiles) return PARSE_ERR_INVALID;
-      // tile-part header markers up to SOD (COD/COC/QCD/QCC inside tile headers unsupported)
+      const bool first = !tile_seen[isot];
+      tile_seen[isot] = true;
+      // precedence inside a tile: tile COC > tile COD > main COC > main COD (likewise QCC/QCD)
+      bool tcoc[J2K_MAX_COMPONENTS] = {false}, tqcc[J2K_MAX_COMPONENTS] = {false};
       for (;;) {
         if (r.left() < 2) return PARSE_ERR_TRUNCATED;
         unsigned mm = r.u16();
         if (mm == 0xFF93) break;
-        if (mm == 0xFF52 || mm == 0xFF53 || mm == 0xFF5C || mm == 0xFF5D || mm == 0xFF5F || mm == 0xFF61)
-          return PARSE_ERR_UNSUPPORTED;
+        if (r.left() < 2) return PARSE_ERR_TRUNCATED;
         unsigned l = r.u16();
         if (l < 2 || l - 2 > r.left()) return PARSE_ERR_TRUNCATED;
+        Reader s{r.p, r.p + (l - 2)};
         r.p += l - 2;
+        int rc = PARSE_OK;
+        const bool coding = mm == 0xFF52 || mm == 0xFF53 || mm == 0xFF5C || mm == 0xFF5D || mm == 0xFF5E;
+        if (coding && !first) continue;  // only the first tile-part may carry them
+        if ((coding || mm == 0xFF5F) && !thdr[isot]) {
+          thdr[isot].reset(new StreamHeader(H));  // the main header's values, POC included
+          thdr[isot]->ppm.clear();
+        }
+        StreamHeader *T = thdr[isot].get();
+        switch (mm) {
+          case 0xFF52: rc = read_cod(s, *T, tcoc); break;
+          case 0xFF53: rc = read_coc(s, *T, tcoc); break;
+          case 0xFF5C: rc = read_qcx(s, false, *T, tqcc); break;
+          case 0xFF5D: rc = read_qcx(s, true, *T, tqcc); break;
+          case 0xFF5E: rc = read_rgn(s, *T); break;
+          case 0xFF5F:  // POC: the tile's volumes (from all its tile-parts) replace the main header's
+            if (!tile_poc[isot]) T->poc.clear();
+            tile_poc[isot] = true;
+            rc = read_poc(s, H.ncomp, T->poc);
+            break;
+          case 0xFF61:  // PPT
+            if (H.has_ppm) return PARSE_ERR_INVALID;
+            if (s.left() < 1) return PARSE_ERR_TRUNCATED;
+            packed[isot].insert(packed[isot].end(), s.p + 1, s.end);
+            has_packed[isot] = 1;
+            break;
+          default:  // PLT, COM and others are skipped
+            break;
+        }
+        if (rc != PARSE_OK) return rc;
+      }
+      if (H.has_ppm) {  // Nppm, then this tile-part's packet headers
+        if (H.ppm.size() - ppm_pos < 4) return PARSE_ERR_INVALID;
+        const uint8_t *q = H.ppm.data() + ppm_pos;
+        const size_t n = ((size_t)q[0] << 24) | ((size_t)q[1] << 16) | ((size_t)q[2] << 8) | q[3];
+        if (H.ppm.size() - ppm_pos - 4 < n) return PARSE_ERR_INVALID;
+        packed[isot].insert(packed[isot].end(), q + 4, q + 4 + n);
+        ppm_pos += 4 + n;
       }
       const uint8_t *body = r.p;
       const uint8_t *tend;
@@ -475,24 +586,38 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       if (psot == 0) break;
     }
   }
+  for (int t = 0; t < ntiles; ++t)
+    if (thdr[t]) {
+      const int rc = finish_coding(*thdr[t], &H);
+      if (rc != PARSE_OK) return rc;
+    }
+  auto tile_header = [&](int t) -> const StreamHeader & { return thdr[t] ? *thdr[t] : H; };
+
+  int discard = opt.discard_levels;
+  for (int t = 0; t < ntiles; ++t)
+    for (int c = 0; c < H.ncomp; ++c) discard = std::min(discard, tile_header(t).levels[c]);
+  if (discard < 0) discard = 0;
+  P.discard = discard;
 
   // ---- geometry and Tier-2 per tile
   uint64_t coef_total = 0;
   P.out_w = ceil_div_pow2(H.width, discard);
   P.out_h = ceil_div_pow2(H.height, discard);
   for (int t = 0; t < ntiles; ++t) {
+    const StreamHeader &TH = tile_header(t);
+    const int maxlayers = opt.max_layers > 0 ? std::min(opt.max_layers, TH.layers) : TH.layers;
     int tx = t % ntx, ty = t / ntx;
-    int tx0 = std::max(H.tx0 + tx * H.tile_w, H.x0), ty0 = std::max(H.ty0 + ty * H.tile_h, H.y0);
-    int tx1 = std::min(H.tx0 + (tx + 1) * H.tile_w, H.width), ty1 = std::min(H.ty0 + (ty + 1) * H.tile_h, H.height);
-    std::vector<TCState> tcs(H.ncomp);
-    for (int c = 0; c < H.ncomp; ++c) {
+    int tx0 = std::max(TH.tx0 + tx * TH.tile_w, TH.x0), ty0 = std::max(TH.ty0 + ty * TH.tile_h, TH.y0);
+    int tx1 = std::min(TH.tx0 + (tx + 1) * TH.tile_w, TH.width), ty1 = std::min(TH.ty0 + (ty + 1) * TH.tile_h, TH.height);
+    std::vector<TCState> tcs(TH.ncomp);
+    for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       TC.comp = c;
       TC.x0 = tx0;
       TC.y0 = ty0;
       TC.x1 = tx1;
       TC.y1 = ty1;
-      TC.levels = H.levels[c];
+      TC.levels = TH.levels[c];
       const int L = TC.levels;
       TC.res.resize(L + 1);
       for (int r = 0; r <= L; ++r) {
@@ -507,15 +632,15 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
         if ((R.x0 & 1) || (R.y0 & 1)) {
           if (r < L) return PARSE_ERR_UNSUPPORTED;
         }
-        int ppx = H.ppx[c][r], ppy = H.ppy[c][r];
+        int ppx = TH.ppx[c][r], ppy = TH.ppy[c][r];
         if (R.x1 > R.x0 && R.y1 > R.y0) {
           R.npx = ((R.x1 + (1 << ppx) - 1) >> ppx) - (R.x0 >> ppx);
           R.npy = ((R.y1 + (1 << ppy) - 1) >> ppy) - (R.y0 >> ppy);
         }
         int nbands = r == 0 ? 1 : 3;
         R.bands.resize(nbands);
-        int cbw = r == 0 ? std::min(H.cbw_exp[c], ppx) : std::min(H.cbw_exp[c], ppx - 1);
-        int cbh = r == 0 ? std::min(H.cbh_exp[c], ppy) : std::min(H.cbh_exp[c], ppy - 1);
+        int cbw = r == 0 ? std::min(TH.cbw_exp[c], ppx) : std::min(TH.cbw_exp[c], ppx - 1);
+        int cbh = r == 0 ? std::min(TH.cbh_exp[c], ppy) : std::min(TH.cbh_exp[c], ppy - 1);
         for (int b = 0; b < nbands; ++b) {
           BandState &B = R.bands[b];
           B.type = r == 0 ? 0 : b + 1;
@@ -529,14 +654,14 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
           B.cbw_exp = cbw;
           B.cbh_exp = cbh;
           int bi = r == 0 ? 0 : 1 + 3 * (r - 1) + b;
-          B.spqcd = H.steps[c][bi];
-          int G = H.guard[c];
-          if (H.reversible[c]) {
+          B.spqcd = TH.steps[c][bi];
+          int G = TH.guard[c];
+          if (TH.reversible[c]) {
             B.mb = (int)B.spqcd + G - 1;
             B.gain = 0.f;
           } else {
-            B.mb = (int)((((uint32_t)B.spqcd) + (uint32_t)G - 1) >> 11);
-            B.gain = irrev_band_gain(B.spqcd, H.depth[c], B.type, L == 0);
+            B.mb = std::max(0, (int)(B.spqcd >> 11) + G - 1);
+            B.gain = irrev_band_gain(B.spqcd, TH.depth[c], B.type, L == 0);
           }
           // position in the Mallat region of the tile-component
           if (r == 0) {
@@ -580,8 +705,8 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
                   cb.w = gx1 - gx0;
                   cb.h = gy1 - gy0;
                   // one piece per contributing layer, usually one segment per layer
-                  cb.pieces.reserve(std::min(H.layers, 16));
-                  cb.seglen.reserve(std::min(H.layers, 16));
+                  cb.pieces.reserve(std::min(TH.layers, 16));
+                  cb.seglen.reserve(std::min(TH.layers, 16));
                   B.prec_cbs[p].push_back((int)B.cbs.size());
                   B.cbs.push_back(std::move(cb));
                 }
@@ -615,19 +740,22 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     };
     std::vector<Contrib> contribs;
     std::vector<uint32_t> lens;
+    // packet headers: in the tile data, or packed (PPM / PPT) in a stream of their own
+    const bool pk = has_packed[t] != 0;
+    const uint8_t *hcur = pk ? packed[t].data() : nullptr;
+    const uint8_t *const hend = pk ? packed[t].data() + packed[t].size() : nullptr;
+    // reads the packet of layer l, resolution r, component c, precinct p (which exist)
     auto read_packet = [&](int l, int r, int c, int p) -> int {
       TCState &TC = tcs[c];
-      if (r > TC.levels) return PARSE_OK;
       ResState &R = TC.res[r];
-      if (p >= R.npx * R.npy) return PARSE_OK;
       if (stream_end) return PARSE_OK;
       while (cur && cur >= end) next_part();
-      if (!cur) {
+      if (pk ? hcur >= hend : !cur) {
         stream_end = true;  // truncated tile: remaining packets are empty
         return PARSE_OK;
       }
-      if (H.sop && end - cur >= 6 && cur[0] == 0xFF && cur[1] == 0x91) cur += 6;
-      BitReader br{cur, end};
+      if (TH.sop && cur && end - cur >= 6 && cur[0] == 0xFF && cur[1] == 0x91) cur += 6;
+      BitReader br = pk ? BitReader{hcur, hend} : BitReader{cur, end};
       contribs.clear();
       lens.clear();
       if (br.bit()) {
@@ -669,11 +797,11 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             int s = cb.passes;
             while (s < cb.passes + n) {
               int e = s + 1;
-              while (e < cb.passes + n && !seg_starts(H.cbstyle[c], e)) ++e;
+              while (e < cb.passes + n && !seg_starts(TH.cbstyle[c], e)) ++e;
               int nb = cb.lblock + floor_log2((uint32_t)(e - s));
               if (nb > 32) return PARSE_ERR_PACKET;
               lens.push_back(br.bits(nb));
-              if (s == cb.passes) ct.first_seg_new = seg_starts(H.cbstyle[c], s);
+              if (s == cb.passes) ct.first_seg_new = seg_starts(TH.cbstyle[c], s);
               s = e;
             }
             if (br.overrun) return PARSE_ERR_PACKET;
@@ -684,10 +812,10 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
         }
       }
       br.align();
-      cur = br.p;
-      if (H.eph) {
-        if (end - cur >= 2 && cur[0] == 0xFF && cur[1] == 0x92) cur += 2;
-      }
+      const uint8_t *&hp = pk ? hcur : cur;
+      const uint8_t *const he = pk ? hend : end;
+      hp = br.p;
+      if (TH.eph && he - hp >= 2 && hp[0] == 0xFF && hp[1] == 0x92) hp += 2;
       const bool keep = l < maxlayers;
       for (auto &ct : contribs) {
         CbState &cb = *ct.cb;
@@ -713,45 +841,90 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       return PARSE_OK;
     };
 
+    // ---- packet order (T.800 B.12): the tile's POC volumes, else the main header's, else
+    // the COD progression over everything.  Each packet is read once: a volume skips the
+    // layers of a precinct that an earlier volume has read.
     int maxL = 0;
-    for (int c = 0; c < H.ncomp; ++c) maxL = std::max(maxL, tcs[c].levels);
-    int maxP = 1;
-    for (int c = 0; c < H.ncomp; ++c)
-      for (auto &R : tcs[c].res) maxP = std::max(maxP, R.npx * R.npy);
-    bool multi_prec = maxP > 1;
-    if (multi_prec && H.progression > 1) return PARSE_ERR_UNSUPPORTED;
+    for (int c = 0; c < TH.ncomp; ++c) maxL = std::max(maxL, tcs[c].levels);
+    std::vector<std::vector<std::vector<int>>> next_layer(TH.ncomp);
+    for (int c = 0; c < TH.ncomp; ++c) {
+      next_layer[c].resize(tcs[c].levels + 1);
+      for (int r = 0; r <= tcs[c].levels; ++r) next_layer[c][r].assign(tcs[c].res[r].npx * tcs[c].res[r].npy, 0);
+    }
+    auto nprec = [&](int r, int c) -> int { return r <= tcs[c].levels ? (int)next_layer[c][r].size() : 0; };
+    auto visit = [&](int l, int r, int c, int p) -> int {
+      int &nl = next_layer[c][r][p];
+      if (l < nl) return PARSE_OK;
+      nl = l + 1;
+      return read_packet(l, r, c, p);
+    };
+    // position-driven orders visit each precinct at the reference-grid point of its
+    // upper-left corner inside the tile (T.800 B.12.1.3-B.12.1.5)
+    struct PrecinctVisit {
+      int64_t y, x;
+      int r, c, p;
+    };
+    std::vector<PrecinctVisit> pv;
+    std::vector<PocEntry> vols = TH.poc;
+    if (vols.empty()) vols.push_back({0, 0, TH.layers, maxL + 1, TH.ncomp, TH.progression});
     int rc = PARSE_OK;
-    switch (H.progression) {
-      case 0:  // LRCP
-        for (int l = 0; l < H.layers && rc == PARSE_OK; ++l)
-          for (int r = 0; r <= maxL && rc == PARSE_OK; ++r)
-            for (int c = 0; c < H.ncomp && rc == PARSE_OK; ++c)
-              for (int p = 0; p < maxP && rc == PARSE_OK; ++p) rc = read_packet(l, r, c, p);
-        break;
-      case 1:  // RLCP
-        for (int r = 0; r <= maxL && rc == PARSE_OK; ++r)
-          for (int l = 0; l < H.layers && rc == PARSE_OK; ++l)
-            for (int c = 0; c < H.ncomp && rc == PARSE_OK; ++c)
-              for (int p = 0; p < maxP && rc == PARSE_OK; ++p) rc = read_packet(l, r, c, p);
-        break;
-      case 2:  // RPCL (one precinct per resolution)
-        for (int r = 0; r <= maxL && rc == PARSE_OK; ++r)
-          for (int c = 0; c < H.ncomp && rc == PARSE_OK; ++c)
-            for (int l = 0; l < H.layers && rc == PARSE_OK; ++l) rc = read_packet(l, r, c, 0);
-        break;
-      case 3:  // PCRL
-      case 4:  // CPRL
-        for (int c = 0; c < H.ncomp && rc == PARSE_OK; ++c)
-          for (int r = 0; r <= maxL && rc == PARSE_OK; ++r)
-            for (int l = 0; l < H.layers && rc == PARSE_OK; ++l) rc = read_packet(l, r, c, 0);
-        break;
-      default:
-        return PARSE_ERR_UNSUPPORTED;
+    for (const PocEntry &v : vols) {
+      const int lye = std::min(v.lye, TH.layers), re = std::min(v.re, maxL + 1), ce = std::min(v.ce, TH.ncomp);
+      const int rs = v.rs, cs = v.cs;
+      if (rs >= re || cs >= ce || lye <= 0) continue;
+      if (v.prog == 0) {  // LRCP
+        for (int l = 0; l < lye && rc == PARSE_OK; ++l)
+          for (int r = rs; r < re && rc == PARSE_OK; ++r)
+            for (int c = cs; c < ce && rc == PARSE_OK; ++c)
+              for (int p = 0; p < nprec(r, c) && rc == PARSE_OK; ++p) rc = visit(l, r, c, p);
+      } else if (v.prog == 1) {  // RLCP
+        for (int r = rs; r < re && rc == PARSE_OK; ++r)
+          for (int l = 0; l < lye && rc == PARSE_OK; ++l)
+            for (int c = cs; c < ce && rc == PARSE_OK; ++c)
+              for (int p = 0; p < nprec(r, c) && rc == PARSE_OK; ++p) rc = visit(l, r, c, p);
+      } else {  // RPCL, PCRL, CPRL
+        pv.clear();
+        for (int c = cs; c < ce; ++c) {
+          const TCState &TC = tcs[c];
+          for (int r = rs; r < re && r <= TC.levels; ++r) {
+            const ResState &R = TC.res[r];
+            if (R.npx * R.npy == 0) continue;
+            const int lv = TC.levels - r, ppx = TH.ppx[c][r], ppy = TH.ppy[c][r];
+            const int64_t rx0 = (int64_t)R.x0 << lv, ry0 = (int64_t)R.y0 << lv;
+            const int64_t spx = (int64_t)1 << (ppx + lv), spy = (int64_t)1 << (ppy + lv);
+            const int px0 = R.x0 >> ppx, py0 = R.y0 >> ppy;
+            for (int pj = 0; pj < R.npy; ++pj) {
+              const int64_t y = pj ? (int64_t)(py0 + pj) * spy : ((ry0 % spy) ? TC.y0 : ry0);
+              for (int pi = 0; pi < R.npx; ++pi) {
+                const int64_t x = pi ? (int64_t)(px0 + pi) * spx : ((rx0 % spx) ? TC.x0 : rx0);
+                pv.push_back({y, x, r, c, pj * R.npx + pi});
+              }
+            }
+          }
+        }
+        const int prog = v.prog;
+        std::sort(pv.begin(), pv.end(), [prog](const PrecinctVisit &a, const PrecinctVisit &b) {
+          if (prog == 2) {  // RPCL: resolution, y, x, component
+            if (a.r != b.r) return a.r < b.r;
+            if (a.y != b.y) return a.y < b.y;
+            if (a.x != b.x) return a.x < b.x;
+            return a.c < b.c;
+          }
+          if (prog == 4 && a.c != b.c) return a.c < b.c;  // CPRL: component first
+          if (a.y != b.y) return a.y < b.y;
+          if (a.x != b.x) return a.x < b.x;
+          if (prog == 3 && a.c != b.c) return a.c < b.c;  // PCRL: y, x, component, resolution
+          return a.r < b.r;
+        });
+        for (const PrecinctVisit &q : pv)
+          for (int l = 0; l < lye && rc == PARSE_OK; ++l) rc = visit(l, q.r, q.c, q.p);
+      }
+      if (rc != PARSE_OK) break;
     }
     if (rc != PARSE_OK) return rc;
 
     // ---- emit plan entries for this tile
-    for (int c = 0; c < H.ncomp; ++c) {
+    for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       if ((opt.ignore_components >> c) & 1) continue;
       const int L = TC.levels;
@@ -783,7 +956,7 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             d.mb = (uint8_t)std::min(B.mb, 255);
             d.missing = (uint8_t)std::min(cb.missing, 255);
             d.num_passes = (uint8_t)cb.kept;
-            d.flags = (uint8_t)((H.cbstyle[c] & 0x3F) | (H.reversible[c] ? 0 : J2K_CB_IRREV));
+            d.flags = (uint8_t)((TH.cbstyle[c] & 0x3F) | (TH.reversible[c] ? 0 : J2K_CB_IRREV));
             d.gain = B.gain;
             d.out_stride = (uint32_t)tc.w;
             d.out_off = tc.coef_off + (uint64_t)(B.off_y + cb.y0) * tc.w + (B.off_x + cb.x0);

@@ -3,8 +3,9 @@
  * Tier-2 packet headers, producing a decode plan (plan.h) for the device.
  *
  * Mirrors the role of the reference's codestream layer, which stays on the host there too:
- * dec_syntax.cpp (SIZ/COD/COC/QCD/QCC/RGN/COM parsing, :134-421), dec_packet.cpp (packet
- * headers, pass counts, Lblock, lengths, :66-221; progression orders :384-730),
+ * dec_syntax.cpp (SIZ/COD/COC/QCD/QCC/RGN/COM/POC/PPM parsing, :134-421; tile-part headers
+ * with COD/COC/QCD/QCC/RGN/POC/PPT, :560-720), dec_packet.cpp (packet headers, pass
+ * counts, Lblock, lengths, :66-221; progression orders :384-830),
  * dec_tagtree.cpp (tag trees), dec_init.cpp (tile / subband / code-block geometry,
  * :645-1056) and dec_jp2.cpp (JP2 wrapper, BMI_dec_info sizes, :420-597).
  */
@@ -35,7 +36,14 @@ struct DecodeOptions {
   unsigned ignore_components = 0; /* bit c set: component c is not decoded */
 };
 
-/* Header-level description (main header only; no Tier-2). */
+/* One progression volume of a POC marker (T.800 A.6.6): layers [0, lye), resolutions
+ * [rs, re), components [cs, ce) in progression order `prog`. */
+struct PocEntry {
+  int rs, cs, lye, re, ce, prog;
+};
+
+/* Coding parameters of the main header, or of one tile (the main header's values with the
+ * tile's own COD / COC / QCD / QCC / POC applied). */
 struct StreamHeader {
   int width = 0, height = 0, x0 = 0, y0 = 0;
   int tile_w = 0, tile_h = 0, tx0 = 0, ty0 = 0;
@@ -54,6 +62,9 @@ struct StreamHeader {
   int guard[J2K_MAX_COMPONENTS] = {0};
   uint16_t steps[J2K_MAX_COMPONENTS][3 * J2K_MAX_LEVELS + 1] = {{0}};  /* raw SPqcd/SPqcc values */
   int roi_shift[J2K_MAX_COMPONENTS] = {0};
+  std::vector<PocEntry> poc;  /* progression volumes (empty: the COD order over everything) */
+  std::vector<uint8_t> ppm;   /* main header only: PPM payloads (Nppm + packed headers per tile-part) */
+  bool has_ppm = false;
   size_t header_len = 0;    /* bytes up to the first SOT */
   size_t cs_offset = 0;     /* offset of SOC inside the input (JP2 wrapper) */
   int ntx() const { return (width - tx0 + tile_w - 1) / tile_w; }

@@ -1323,6 +1323,17 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
   }
 
   // ---------------- codestream
+  const int markers = P->markers;
+  const bool packed_hdrs = (markers & (J2KENC_PPM | J2KENC_PPT)) != 0;
+  const int nparts = P->tile_parts > 1 ? P->tile_parts : 1;
+  if ((markers & J2KENC_PPM) && (markers & J2KENC_PPT)) return -11;
+  if (nparts > 255 || P->num_poc < 0 || P->num_poc > 8) return -11;
+  for (int i = 0; i < P->num_poc; ++i) {
+    const int *v = P->poc[i];
+    if (v[0] < 0 || v[0] >= v[3] || v[3] > L + 1 || v[1] < 0 || v[1] >= v[4] || v[4] > ncomp || v[2] < 1 ||
+        v[2] > NL || v[5] < 0 || v[5] > 4)
+      return -11;
+  }
   std::vector<uint8_t> cs;
   cs.reserve(1 << 20);
   put_u16(cs, 0xFF4F);  // SOC
@@ -1347,7 +1358,7 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
   // COD
   put_u16(cs, 0xFF52);
   put_u16(cs, 12);
-  cs.push_back(0);  // Scod: default precincts, no SOP/EPH
+  cs.push_back((uint8_t)(((markers & J2KENC_SOP) ? 2 : 0) | ((markers & J2KENC_EPH) ? 4 : 0)));  // Scod
   cs.push_back((uint8_t)P->progression);
   put_u16(cs, NL);
   cs.push_back(mct ? 1 : 0);
@@ -1376,6 +1387,11 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
     cs.insert(cs.end(), msg, msg + sizeof(msg) - 1);
   }
 
+  // tile-parts of every tile: header markers, body, and the packed packet headers (PPM / PPT)
+  struct TilePart {
+    std::vector<uint8_t> markers, body, packed;
+  };
+  std::vector<std::vector<TilePart>> tparts(tiles.size());
   for (int t = 0; t < (int)tiles.size(); ++t) {
     Tile &T = tiles[t];
     // reset T2 state
@@ -1417,7 +1433,10 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
         }
       }
     }
-    std::vector<uint8_t> body;
+    struct Packet {
+      std::vector<uint8_t> hdr, body;
+    };
+    std::vector<Packet> pkts;
     auto emit_packet = [&](int l, int r, int c) {
       Resolution &R = T.comps[c].res[r];
       if (R.x1 <= R.x0 || R.y1 <= R.y0) return;  // no precinct
@@ -1485,43 +1504,144 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
         }
       }
       bw.flush();
-      body.insert(body.end(), hdr.begin(), hdr.end());
-      for (auto &pc : pieces) body.insert(body.end(), pc.first, pc.first + pc.second);
+      Packet pk;
+      pk.hdr = std::move(hdr);
+      for (auto &pc : pieces) pk.body.insert(pk.body.end(), pc.first, pc.first + pc.second);
+      pkts.push_back(std::move(pk));
     };
-    switch (P->progression) {
-      case J2KENC_LRCP:
-        for (int l = 0; l < NL; ++l)
-          for (int r = 0; r <= L; ++r)
-            for (int c = 0; c < ncomp; ++c) emit_packet(l, r, c);
-        break;
-      case J2KENC_RLCP:
-        for (int r = 0; r <= L; ++r)
-          for (int l = 0; l < NL; ++l)
-            for (int c = 0; c < ncomp; ++c) emit_packet(l, r, c);
-        break;
-      case J2KENC_RPCL:
-        for (int r = 0; r <= L; ++r)
-          for (int c = 0; c < ncomp; ++c)
-            for (int l = 0; l < NL; ++l) emit_packet(l, r, c);
-        break;
-      case J2KENC_PCRL:
-      case J2KENC_CPRL:
-        for (int c = 0; c < ncomp; ++c)
-          for (int r = 0; r <= L; ++r)
-            for (int l = 0; l < NL; ++l) emit_packet(l, r, c);
-        break;
-      default:
-        return -8;
+    // packet order: the progression volumes, each packet once (T.800 B.12)
+    std::vector<std::vector<int>> next_layer(ncomp, std::vector<int>(L + 1, 0));
+    auto visit = [&](int l, int r, int c) {
+      if (next_layer[c][r] != l) return;
+      next_layer[c][r] = l + 1;
+      emit_packet(l, r, c);
+    };
+    std::vector<std::vector<int>> vols;
+    for (int i = 0; i < P->num_poc; ++i) vols.push_back(std::vector<int>(P->poc[i], P->poc[i] + 6));
+    if (vols.empty()) vols.push_back({0, 0, NL, L + 1, ncomp, P->progression});
+    for (auto &v : vols) {
+      const int rs = v[0], c0 = v[1], lye = v[2], re = v[3], ce = v[4];
+      switch (v[5]) {
+        case J2KENC_LRCP:
+          for (int l = 0; l < lye; ++l)
+            for (int r = rs; r < re; ++r)
+              for (int c = c0; c < ce; ++c) visit(l, r, c);
+          break;
+        case J2KENC_RLCP:
+          for (int r = rs; r < re; ++r)
+            for (int l = 0; l < lye; ++l)
+              for (int c = c0; c < ce; ++c) visit(l, r, c);
+          break;
+        case J2KENC_RPCL:
+          for (int r = rs; r < re; ++r)
+            for (int c = c0; c < ce; ++c)
+              for (int l = 0; l < lye; ++l) visit(l, r, c);
+          break;
+        default:  // PCRL, CPRL: one precinct per resolution, all at the tile origin
+          for (int c = c0; c < ce; ++c)
+            for (int r = rs; r < re; ++r)
+              for (int l = 0; l < lye; ++l) visit(l, r, c);
+          break;
+      }
     }
-    // SOT + SOD + body
+    for (int c = 0; c < ncomp; ++c)
+      for (int r = 0; r <= L; ++r)
+        if (next_layer[c][r] != NL) return -10;  // the volumes leave packets out
+    // tile-parts: SOP before each packet, EPH after each header, headers packed or inline
+    const size_t n = pkts.size();
+    int zppt = 0;
+    for (int k = 0; k < nparts; ++k) {
+      TilePart tp;
+      for (size_t i = k * n / nparts; i < (k + 1) * n / nparts; ++i) {
+        if (markers & J2KENC_SOP) {
+          put_u16(tp.body, 0xFF91);
+          put_u16(tp.body, 4);
+          put_u16(tp.body, (unsigned)(i & 0xFFFF));
+        }
+        std::vector<uint8_t> &h = packed_hdrs ? tp.packed : tp.body;
+        h.insert(h.end(), pkts[i].hdr.begin(), pkts[i].hdr.end());
+        if (markers & J2KENC_EPH) put_u16(h, 0xFF92);
+        tp.body.insert(tp.body.end(), pkts[i].body.begin(), pkts[i].body.end());
+      }
+      if (k == 0 && P->num_poc && P->poc_in_tiles) {
+        put_u16(tp.markers, 0xFF5F);
+        put_u16(tp.markers, (unsigned)(2 + 7 * P->num_poc));
+        for (int i = 0; i < P->num_poc; ++i) {
+          const int *v = P->poc[i];
+          tp.markers.push_back((uint8_t)v[0]);
+          tp.markers.push_back((uint8_t)v[1]);
+          put_u16(tp.markers, (unsigned)v[2]);
+          tp.markers.push_back((uint8_t)v[3]);
+          tp.markers.push_back((uint8_t)v[4]);
+          tp.markers.push_back((uint8_t)v[5]);
+        }
+      }
+      if (markers & J2KENC_PPT) {  // PPT segments of at most 65532 header bytes
+        size_t off = 0;
+        do {
+          const size_t m = std::min<size_t>(65532, tp.packed.size() - off);
+          if (zppt > 255) return -12;
+          put_u16(tp.markers, 0xFF61);
+          put_u16(tp.markers, (unsigned)(3 + m));
+          tp.markers.push_back((uint8_t)zppt++);
+          tp.markers.insert(tp.markers.end(), tp.packed.begin() + off, tp.packed.begin() + off + m);
+          off += m;
+        } while (off < tp.packed.size());
+      }
+      tparts[t].push_back(std::move(tp));
+    }
+  }
+  // codestream order of the tile-parts
+  std::vector<std::pair<int, int>> order;
+  if (P->interleave_tile_parts) {
+    for (int k = 0; k < nparts; ++k)
+      for (int t = 0; t < (int)tiles.size(); ++t) order.push_back({t, k});
+  } else {
+    for (int t = 0; t < (int)tiles.size(); ++t)
+      for (int k = 0; k < nparts; ++k) order.push_back({t, k});
+  }
+  if (P->num_poc && !P->poc_in_tiles) {  // main-header POC
+    put_u16(cs, 0xFF5F);
+    put_u16(cs, (unsigned)(2 + 7 * P->num_poc));
+    for (int i = 0; i < P->num_poc; ++i) {
+      const int *v = P->poc[i];
+      cs.push_back((uint8_t)v[0]);
+      cs.push_back((uint8_t)v[1]);
+      put_u16(cs, (unsigned)v[2]);
+      cs.push_back((uint8_t)v[3]);
+      cs.push_back((uint8_t)v[4]);
+      cs.push_back((uint8_t)v[5]);
+    }
+  }
+  if (markers & J2KENC_PPM) {  // Nppm + headers of every tile-part, in codestream order
+    std::vector<uint8_t> ppm;
+    for (auto &o : order) {
+      const TilePart &tp = tparts[o.first][o.second];
+      put_u32(ppm, (uint32_t)tp.packed.size());
+      ppm.insert(ppm.end(), tp.packed.begin(), tp.packed.end());
+    }
+    size_t off = 0;
+    for (int z = 0; off < ppm.size(); ++z) {
+      if (z > 255) return -12;
+      const size_t m = std::min<size_t>(65532, ppm.size() - off);
+      put_u16(cs, 0xFF60);
+      put_u16(cs, (unsigned)(3 + m));
+      cs.push_back((uint8_t)z);
+      cs.insert(cs.end(), ppm.begin() + off, ppm.begin() + off + m);
+      off += m;
+    }
+  }
+  for (auto &o : order) {  // SOT + tile-part header markers + SOD + body
+    const TilePart &tp = tparts[o.first][o.second];
     put_u16(cs, 0xFF90);
     put_u16(cs, 10);
-    put_u16(cs, (unsigned)t);
-    put_u32(cs, (uint32_t)(12 + 2 + body.size()));
-    cs.push_back(0);
-    cs.push_back(1);
+    put_u16(cs, (unsigned)o.first);
+    put_u32(cs, (uint32_t)(12 + tp.markers.size() + 2 + tp.body.size()));
+    cs.push_back((uint8_t)o.second);
+    cs.push_back((uint8_t)nparts);
+    cs.insert(cs.end(), tp.markers.begin(), tp.markers.end());
     put_u16(cs, 0xFF93);
-    cs.insert(cs.end(), body.begin(), body.end());
+    cs.insert(cs.end(), tp.body.begin(), tp.body.end());
   }
   put_u16(cs, 0xFFD9);  // EOC
   *out = (uint8_t *)std::malloc(cs.size());

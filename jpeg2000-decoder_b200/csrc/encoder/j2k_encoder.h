@@ -6,7 +6,9 @@
  * synthetic images.  Supported: reversible 5/3 + RCT, irreversible 9/7 + ICT with
  * scalar-expounded quantisation, rectangular tiles anchored at the origin, 32/64 code-blocks,
  * quality layers chosen by slope thresholds, LRCP/RLCP/RPCL/PCRL/CPRL progression with one
- * precinct per resolution, and the BYPASS / RESET / TERMALL / SEGSYM mode switches.
+ * precinct per resolution, progression volumes (POC, main or tile-part header), tile-parts
+ * (optionally interleaved across tiles), SOP / EPH markers, packed packet headers (PPM or
+ * PPT), and the BYPASS / RESET / TERMALL / SEGSYM mode switches.
  *
  * The irreversible path writes one guard bit by default: the reference's Tier-1 places the
  * most significant magnitude bit at (expn - 1 - missing) (decoder/codec/src/
@@ -34,6 +36,9 @@ enum j2kenc_mode {
   J2KENC_SEGSYM = 0x20
 };
 
+/* marker options (T.800 A.6.1 Scod, A.7.4-A.7.5, A.8) */
+enum j2kenc_marker { J2KENC_SOP = 1, J2KENC_EPH = 2, J2KENC_PPM = 4, J2KENC_PPT = 8 };
+
 typedef struct j2kenc_params {
   int reversible;     /* 1: 5/3 integer + RCT; 0: 9/7 + ICT */
   int levels;         /* decomposition levels, 0..10 */
@@ -49,6 +54,13 @@ typedef struct j2kenc_params {
   int guard_bits;     /* 0: 1 for 9/7, 2 for 5/3 */
   double base_step;   /* 9/7: quantiser step for a unit-energy band, in sample units */
   int num_threads;    /* 0: hardware concurrency */
+  int markers;        /* OR of j2kenc_marker (PPM and PPT exclude each other) */
+  int tile_parts;     /* tile-parts per tile, packets split evenly (0 or 1: one) */
+  int interleave_tile_parts; /* write part k of every tile before part k + 1 */
+  int num_poc;        /* progression volumes (0: the COD progression); they must cover every packet */
+  int poc[8][6];      /* per volume: first resolution, first component, layer end, resolution end,
+                         component end, progression */
+  int poc_in_tiles;   /* 0: POC in the main header; 1: in the first tile-part header of each tile */
 } j2kenc_params;
 
 void j2kenc_default_params(j2kenc_params *p);

@@ -45,7 +45,8 @@ typedef struct j2k_cblk {
   uint8_t num_passes;  /* coding passes included over all layers */
   uint8_t missing;     /* zero (missing) most significant bit-planes */
   uint8_t band;        /* 0 LL, 1 HL, 2 LH, 3 HH */
-  uint8_t mb;          /* reference "numbps": SPqcd exponent + guard bits - 1 */
+  uint8_t mb;          /* magnitude bit-planes M_b = exponent + guard bits - 1 (T.800 E.1.1.1; the
+                          reference's "numbps" for one guard bit) */
   uint8_t flags;       /* J2K_CB_* */
   uint8_t nseg;        /* codeword segments (>= 1 when num_passes > 0) */
   uint16_t spqcd;      /* raw QCD/QCC step value of the band (exponent << 11 | mantissa, or exponent) */

@@ -36,6 +36,7 @@ J2K_ERR_DECODE = -7
 J2K_ERR_TIMEOUT = -6
 J2K_ERR_NOMEM = -5
 J2K_ERR_STATE = -8
+J2K_ERR_UNSUPPORTED = -3
 
 
 class J2kError(RuntimeError):
@@ -89,7 +90,11 @@ class EncParams(ctypes.Structure):
                 ("cbh_exp", ctypes.c_int), ("tile_w", ctypes.c_int), ("tile_h", ctypes.c_int),
                 ("num_layers", ctypes.c_int), ("layer_bpp", ctypes.c_double * 32), ("progression", ctypes.c_int),
                 ("mode", ctypes.c_int), ("use_mct", ctypes.c_int), ("guard_bits", ctypes.c_int),
-                ("base_step", ctypes.c_double), ("num_threads", ctypes.c_int)]
+                ("base_step", ctypes.c_double), ("num_threads", ctypes.c_int), ("markers", ctypes.c_int),
+                ("tile_parts", ctypes.c_int), ("interleave_tile_parts", ctypes.c_int), ("num_poc", ctypes.c_int),
+                ("poc", (ctypes.c_int * 6) * 8), ("poc_in_tiles", ctypes.c_int)]
+
+ENC_SOP, ENC_EPH, ENC_PPM, ENC_PPT = 1, 2, 4, 8
 
 
 assert ctypes.sizeof(CodeBlock) == 40
@@ -226,6 +231,11 @@ def encode(planes, bitdepth, **kw):
         if k == "layer_bpp":
             for n, x in enumerate(v):
                 p.layer_bpp[n] = float(x)
+        elif k == "poc":  # list of (RS, CS, LYE, RE, CE, progression)
+            p.num_poc = len(v)
+            for n, e in enumerate(v):
+                for j, x in enumerate(e):
+                    p.poc[n][j] = int(x)
         else:
             setattr(p, k, v)
     a = np.ascontiguousarray(planes, dtype=np.uint16)

@@ -1,0 +1,113 @@
+"""Host Tier-2 front end on streams beyond the benchmark configurations (CPU only).
+
+Every stream is planned by the library (j2k_plan_create) and decoded by the oracle from that
+plan; the checks are the lossless identity with the source picture, or, for the 9/7
+fixture written by OpenJPEG, agreement with OpenJPEG's own decode within one level.
+Covered: several precincts per resolution under all five progression orders (T.800
+B.12.1.1-B.12.1.5), precinct-limited code-block sizes, POC volumes in the main and tile-part
+headers, PPM / PPT packed packet headers, SOP / EPH markers, tile-parts (also interleaved
+across tiles), tile-part COD / QCD overriding the main header, and the T.800 magnitude bit
+count for 9/7 bands with two guard bits (E.1.1.1).
+"""
+import io
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_util
+import tier2_streams as ts
+from conftest import ROOT
+
+FIX = os.path.join(ROOT, "tests", "golden", "tier2")
+
+
+@pytest.fixture(scope="module")
+def pkg():
+    from conftest import load_package
+    return load_package()
+
+
+def _manifest():
+    with open(os.path.join(FIX, "manifest.json")) as f:
+        return json.load(f)
+
+
+def _oracle_rgb(cs, h, w):
+    from jpeg2000_decoder_b200 import native
+    plan = native.Plan(cs)
+    rc, out, _ = oracle_util.oracle_decode(plan, native.FMT_24BITS_RGB)
+    assert rc == 0
+    return out.reshape(h, w, 3)[:, :, ::-1]
+
+
+@pytest.mark.parametrize("name", sorted(_manifest()["streams"]))
+def test_openjpeg_precinct_fixtures(pkg, name):
+    man = _manifest()
+    exp = np.load(os.path.join(FIX, "expected.npz"))
+    spec = man["streams"][name]
+    with open(os.path.join(FIX, name), "rb") as f:
+        cs = f.read()
+    rgb = _oracle_rgb(cs, man["height"], man["width"]).astype(int)
+    want = exp[spec["expect"]].astype(int)
+    tol = spec.get("tolerance", 0)
+    assert np.abs(rgb - want).max() <= tol, name
+
+
+@pytest.mark.parametrize("case", ts.marker_cases(), ids=lambda c: c[0])
+def test_marker_variants_lossless(pkg, case):
+    name, kw, openjpeg_agrees = case
+    cs = ts.encode_case(kw)
+    src = ts.source()
+    rgb = _oracle_rgb(cs, ts.H, ts.W)
+    assert np.array_equal(rgb.transpose(2, 0, 1), src), name
+    if openjpeg_agrees:  # the stream itself is valid: an independent decoder reads it
+        Image = pytest.importorskip("PIL.Image")
+        ref = np.asarray(Image.open(io.BytesIO(cs)).convert("RGB"))
+        assert np.array_equal(ref.transpose(2, 0, 1), src), name
+
+
+@pytest.mark.parametrize("case", ts.splice_cases(), ids=lambda c: c[0])
+def test_tile_header_coding_overrides(pkg, case):
+    name, cs = case
+    rgb = _oracle_rgb(cs, ts.H, ts.W)
+    assert np.array_equal(rgb.transpose(2, 0, 1), ts.source()), name
+    Image = pytest.importorskip("PIL.Image")
+    ref = np.asarray(Image.open(io.BytesIO(cs)).convert("RGB"))
+    assert np.array_equal(ref.transpose(2, 0, 1), ts.source()), name
+
+
+def test_refusals(pkg):
+    """A tile that switches the wavelet, POC with a broken length, PPM and PPT together."""
+    from jpeg2000_decoder_b200 import native
+    with pytest.raises(native.J2kError) as e:
+        native.Plan(ts.transform_mismatch_stream())
+    assert e.value.code == native.J2K_ERR_UNSUPPORTED
+    cs = bytearray(ts.encode_case(dict(poc=[(0, 0, 3, 4, 3, 0)])))
+    i = cs.find(b"\xff\x5f")
+    cs[i + 3] += 1  # Lpoc no longer a whole number of entries
+    with pytest.raises(native.J2kError):
+        native.Plan(bytes(cs))
+    ppm = ts.encode_case(dict(markers=native.ENC_PPM))
+    ppt = ts.encode_case(dict(markers=native.ENC_PPT))
+    segs, sot = ts._segments(ppm, 2)
+    with pytest.raises(native.J2kError):
+        native.Plan(ppm[:sot] + ppt[ts._segments(ppt, 2)[1]:])
+
+
+def test_cinema_profile_poc_and_tile_parts(pkg):
+    """OpenJPEG's 2K digital-cinema profile: CPRL, precincts, 32x32 blocks, two guard
+    bits, a POC in the first tile-part header, TLM and one tile-part per resolution."""
+    Image = pytest.importorskip("PIL.Image")
+    from jpeg2000_decoder_b200 import native, synth
+    src = np.ascontiguousarray(np.moveaxis(synth.fields_and_edges(12, 1080, 2048).astype(np.uint8), 0, -1))
+    f = io.BytesIO()
+    Image.fromarray(src, "RGB").save(f, "JPEG2000", no_jp2=True, cinema_mode="cinema2k-24")
+    cs = f.getvalue()
+    assert b"\xff\x5f" in cs  # POC present
+    plan = native.Plan(cs)
+    assert plan.info.progression == 4 and plan.info.guard_bits == 2
+    rgb = _oracle_rgb(cs, 1080, 2048).astype(int)
+    ref = np.asarray(Image.open(io.BytesIO(cs)).convert("RGB")).astype(int)
+    assert np.abs(rgb - ref).max() <= 1

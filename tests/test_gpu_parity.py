@@ -371,3 +371,29 @@ def test_tiny_and_odd_geometries_bit_exact(gpu_ctx, h, w):
                           else out.reshape(h, w, 4)[:, :, 3][None])
                     assert np.array_equal(px, img)
     gpu_ctx.set_tuning()
+
+
+def test_tier2_variants_bit_exact(gpu_ctx):
+    """Streams beyond the benchmark configurations (several precincts under all progression
+    orders with 2x2..8x8 code-blocks, 9/7 with two guard bits, POC, PPM/PPT, SOP/EPH,
+    tile-parts, tile-header COD/QCD) decode on the device exactly as the oracle decodes
+    their plans; the lossless ones reproduce their source pictures."""
+    from jpeg2000_decoder_b200 import native
+    import tier2_streams as ts
+    fix = os.path.join(GOLDEN, "tier2")
+    with open(os.path.join(fix, "manifest.json")) as f:
+        man = json.load(f)
+    src_fix = np.load(os.path.join(fix, "expected.npz"))["source"].transpose(2, 0, 1)
+    streams = []
+    for name, spec in sorted(man["streams"].items()):
+        with open(os.path.join(fix, name), "rb") as f:
+            streams.append((name, f.read(), src_fix if spec["expect"] == "source" else None))
+    for name, kw, _ in ts.marker_cases():
+        streams.append((name, ts.encode_case(kw), ts.source()))
+    for name, cs in ts.splice_cases():
+        streams.append((name, cs, ts.source()))
+    for name, cs, src in streams:
+        out, plan = _decode_check(gpu_ctx, cs, native.FMT_24BITS_RGB)
+        if src is not None:
+            I = plan.info
+            assert np.array_equal(ts.as_rgb(out, I.height, I.width), src), name
