@@ -267,9 +267,8 @@ def run_gpu(args, rank, world, dist):
     # buffers (enqueued behind the decode, so they overlap the host's next step).  Two
     # contexts alternate, so the host work of one step overlaps the device decode of the
     # previous one, as a decoding service would run; the time is the wall clock from the
-    # first step's parse to the last step's pictures on the host.  Each step's kernels wait
-    # for the previous step's decode to end (its staging copy does not): the persistent
-    # Tier-1 kernel would otherwise hold every SM and delay the previous step's DWT levels.
+    # first step's parse to the last step's pictures on the host.  (The library starts a
+    # step whose Tier-1 fills the GPU after the previous step's decode; smaller ones overlap.)
     import torch
     ctx2 = native.GpuContext(dev)
     ctxs = [ctx, ctx2]
@@ -283,7 +282,6 @@ def run_gpu(args, rank, world, dist):
 
     def e2e_run(nsteps):
         pending = None
-        decoded = None
         for it in range(nsteps):
             k = it % 2
             t0 = time.perf_counter()
@@ -292,12 +290,7 @@ def run_gpu(args, rank, world, dist):
             ctxs[k].begin()
             for p in ps:
                 ctxs[k].add(p, fmt)
-            ctxs[k].stage(e2e_sp[k])
-            if decoded is not None:
-                e2e_streams[k].wait_event(decoded)
-            ctxs[k].run(e2e_sp[k])
-            decoded = torch.cuda.Event()
-            decoded.record(e2e_streams[k])
+            ctxs[k].launch(e2e_sp[k])
             for i, o in enumerate(outs[k]):
                 ctxs[k].output_async(i, o.data_ptr(), o.numel())
             t2 = time.perf_counter()

@@ -23,6 +23,7 @@
 #include <new>
 #include <thread>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "../../include/j2k_gpu.h"
@@ -956,6 +957,21 @@ bool capture_decode(j2k_gpu_ctx *c, cudaStream_t st) {
   c->graph_launches = c->launches;
   return true;
 }
+
+// Order of decodes on one device, across contexts.  Every run records `last` after its
+// decode; a run whose Tier-1 launch fills every SM waits for it first.  The persistent
+// Tier-1 kernel holds its SMs until its queue drains, so if it started while an earlier
+// batch (of any context) was still in its Tier-1 tail, that batch's DWT levels could not
+// run until this whole Tier-1 had finished.  Smaller Tier-1 launches leave SMs free and
+// overlap the previous decode instead, which fills the idle SMs of latency-bound batches.
+struct DeviceOrder {
+  std::mutex mu;
+  cudaEvent_t last = nullptr;
+};
+DeviceOrder &device_order(int device) {
+  static DeviceOrder orders[64];
+  return orders[device & 63];
+}
 }  // namespace
 
 extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
@@ -964,6 +980,10 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   cudaSetDevice(c->device);
   cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
   c->user_stream = st;
+  DeviceOrder &order = device_order(c->device);
+  std::lock_guard<std::mutex> lk(order.mu);
+  if (!order.last) CK(cudaEventCreateWithFlags(&order.last, cudaEventDisableTiming));
+  if ((long long)c->sg.n_cblks >= (long long)c->sm_count * 32) CK(cudaStreamWaitEvent(st, order.last, 0));
   if (c->launched) {
     // a repeated run: no input copies, both copy events at the start
     CK(cudaEventRecord(c->ev[0], st));
@@ -976,6 +996,7 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
     const int rc = enqueue_decode(c, st, false);
     if (rc != J2K_OK) return rc;
   }
+  CK(cudaEventRecord(order.last, st));
   c->launched = true;
   c->synced = false;
   c->copies_pending = false;

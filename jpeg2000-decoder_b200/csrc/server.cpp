@@ -13,10 +13,8 @@
 // and sleeps on the submit condition only when neither step had work.  Requests that
 // arrive while batches run therefore join the next free slot, and up to `pipeline_depth`
 // batches overlap on the device (staging and output copies of one with the kernels of
-// another).  The kernels of consecutive batches run in launch order: each slot's decode
-// waits for the previous batch's decode to end.  Tier-1 is a persistent kernel that holds
-// every SM until its queue drains, so a Tier-1 launched early would keep the previous
-// batch's DWT levels (and with them its output copies) waiting for its whole duration.
+// another; the engine starts a batch whose Tier-1 fills the GPU only after the previous
+// decode, see j2k_gpu_batch_run).
 #include "../../include/j2k_server.h"
 
 #include <cuda_runtime.h>
@@ -89,8 +87,7 @@ struct PinnedPool {
 struct Slot {
   j2k_gpu_ctx *ctx = nullptr;
   cudaStream_t stream = nullptr;
-  cudaEvent_t done_ev = nullptr;     // end of the decode and of the output copies
-  cudaEvent_t decoded_ev = nullptr;  // end of the decode kernels
+  cudaEvent_t done_ev = nullptr;  // end of the decode and of the output copies
   std::vector<Request *> reqs;
   bool busy = false;
 };
@@ -126,7 +123,6 @@ struct j2k_server {
   uint64_t pool_growths = 0, pinned_allocs = 0;
   Clock::time_point busy_since;
   int inflight = 0;
-  Slot *last_run = nullptr;  // the slot whose decode was enqueued last
 
   void run();
   bool complete_ready();
@@ -143,13 +139,7 @@ int j2k_server::launch(Slot &s, std::vector<Request *> &batch) {
   size_t before = 0, after = 0, budget = 0;
   j2k_gpu_mem_usage(s.ctx, &before, &budget);
   const Clock::time_point t0 = Clock::now();
-  if (rc == J2K_OK) rc = j2k_gpu_batch_stage(s.ctx, s.stream);
-  if (rc == J2K_OK && last_run && last_run != &s &&
-      cudaStreamWaitEvent(s.stream, last_run->decoded_ev, 0) != cudaSuccess)
-    rc = J2K_ERR_CUDA;
-  if (rc == J2K_OK) rc = j2k_gpu_batch_run(s.ctx, s.stream);
-  if (rc == J2K_OK && cudaEventRecord(s.decoded_ev, s.stream) != cudaSuccess) rc = J2K_ERR_CUDA;
-  if (rc == J2K_OK) last_run = &s;
+  if (rc == J2K_OK) rc = j2k_gpu_batch_launch(s.ctx, s.stream);
   const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
   j2k_gpu_mem_usage(s.ctx, &after, &budget);
   {
@@ -329,8 +319,6 @@ extern "C" int j2k_server_create(const j2k_server_config *cfg, j2k_server **out)
     int rc = j2k_gpu_ctx_create(s->cfg.device, s->slot_budget, &sl.ctx);
     if (rc == J2K_OK && cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess) rc = J2K_ERR_CUDA;
     if (rc == J2K_OK && cudaEventCreateWithFlags(&sl.done_ev, cudaEventDisableTiming) != cudaSuccess) rc = J2K_ERR_CUDA;
-    if (rc == J2K_OK && cudaEventCreateWithFlags(&sl.decoded_ev, cudaEventDisableTiming) != cudaSuccess)
-      rc = J2K_ERR_CUDA;
     if (rc != J2K_OK) {
       j2k_server_destroy(s);
       return rc;
@@ -364,7 +352,6 @@ extern "C" void j2k_server_destroy(j2k_server *s) {
     if (sl.ctx) j2k_gpu_ctx_destroy(sl.ctx);
     if (sl.stream) cudaStreamDestroy(sl.stream);
     if (sl.done_ev) cudaEventDestroy(sl.done_ev);
-    if (sl.decoded_ev) cudaEventDestroy(sl.decoded_ev);
   }
   for (auto &kv : s->reqs) {
     if (kv.second->plan) j2k_plan_destroy(kv.second->plan);
