@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <mutex>
 #include <cstring>
 
 namespace j2k {
@@ -485,9 +486,46 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   return PARSE_OK;
 }
 
+namespace {
+constexpr size_t kPoolMinBytes = size_t(1) << 20, kPoolMaxBytes = size_t(512) << 20;
+constexpr size_t kPoolMaxBuffers = 8;
+std::mutex g_pool_mu;
+std::vector<std::vector<uint8_t>> g_pool;
+size_t g_pool_bytes = 0;
+}  // namespace
+
+std::vector<uint8_t> take_plan_bytes(size_t capacity) {
+  std::vector<uint8_t> v;
+  if (capacity >= kPoolMinBytes) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    size_t best = g_pool.size();
+    for (size_t i = 0; i < g_pool.size(); ++i)
+      if (g_pool[i].capacity() >= capacity && (best == g_pool.size() || g_pool[i].capacity() < g_pool[best].capacity()))
+        best = i;
+    if (best < g_pool.size()) {
+      v = std::move(g_pool[best]);
+      g_pool.erase(g_pool.begin() + (std::ptrdiff_t)best);
+      g_pool_bytes -= v.capacity();
+      v.clear();
+      return v;
+    }
+    capacity += capacity / 8;  // room for a slightly larger picture when it comes back
+  }
+  v.reserve(capacity);
+  return v;
+}
+
+void give_plan_bytes(std::vector<uint8_t> &&bytes) {
+  if (bytes.capacity() < kPoolMinBytes) return;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (g_pool.size() >= kPoolMaxBuffers || g_pool_bytes + bytes.capacity() > kPoolMaxBytes) return;
+  g_pool_bytes += bytes.capacity();
+  g_pool.push_back(std::move(bytes));
+}
+
 int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImagePlan &P) {
   P = ImagePlan();
-  P.bytes.reserve(len);  // the coded bytes of every block are a subset of the codestream
+  P.bytes = take_plan_bytes(len);  // the coded bytes of every block are a subset of the codestream
   int st = parse_header(data, len, P.hdr);
   if (st != PARSE_OK) return st;
   const StreamHeader &H = P.hdr;

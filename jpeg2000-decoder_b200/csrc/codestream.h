@@ -84,6 +84,13 @@ struct ImagePlan {
 };
 
 int parse_header(const uint8_t *data, size_t len, StreamHeader &hdr);
+/* Plan byte buffers of large pictures are recycled between plans (the coded bytes of a 4K
+ * lossless picture fill tens of MB; a fresh buffer that size costs a page fault per 4 KB on
+ * its first write, about a quarter of the Tier-2 time).  take_plan_bytes returns an empty
+ * buffer with at least `capacity` bytes reserved; give_plan_bytes hands a plan's buffer back
+ * (kept while the pool holds fewer than 8 buffers and under 512 MB). */
+std::vector<uint8_t> take_plan_bytes(size_t capacity);
+void give_plan_bytes(std::vector<uint8_t> &&bytes);
 int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImagePlan &plan);
 const char *status_string(int status);
 

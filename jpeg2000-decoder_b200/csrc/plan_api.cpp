@@ -3,6 +3,7 @@
  * Host-only: it owns the Tier-2 result; the device code only ever sees the flat arrays.
  */
 #include <new>
+#include <utility>
 
 #include "../../include/j2k_gpu.h"
 #include "codestream.h"
@@ -26,7 +27,11 @@ extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels
   return J2K_OK;
 }
 
-extern "C" void j2k_plan_destroy(j2k_plan *p) { delete p; }
+extern "C" void j2k_plan_destroy(j2k_plan *p) {
+  if (!p) return;
+  j2k::give_plan_bytes(std::move(p->p.bytes));
+  delete p;
+}
 
 extern "C" int j2k_plan_info(const j2k_plan *p, j2k_image_info *info) {
   if (!p || !info) return J2K_ERR_ARG;
