@@ -980,10 +980,15 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   cudaSetDevice(c->device);
   cudaStream_t st = user_stream ? (cudaStream_t)user_stream : c->stream;
   c->user_stream = st;
+  // a stream the caller is capturing into a graph of its own gets no cross-capture
+  // dependency: the caller's graph orders its work
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(st, &cap));
+  const bool ordered = cap == cudaStreamCaptureStatusNone;
   DeviceOrder &order = device_order(c->device);
   std::lock_guard<std::mutex> lk(order.mu);
   if (!order.last) CK(cudaEventCreateWithFlags(&order.last, cudaEventDisableTiming));
-  if ((long long)c->sg.n_cblks >= (long long)c->sm_count * 32) CK(cudaStreamWaitEvent(st, order.last, 0));
+  if (ordered && (long long)c->sg.n_cblks >= (long long)c->sm_count * 32) CK(cudaStreamWaitEvent(st, order.last, 0));
   if (c->launched) {
     // a repeated run: no input copies, both copy events at the start
     CK(cudaEventRecord(c->ev[0], st));
@@ -996,7 +1001,7 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
     const int rc = enqueue_decode(c, st, false);
     if (rc != J2K_OK) return rc;
   }
-  CK(cudaEventRecord(order.last, st));
+  if (ordered) CK(cudaEventRecord(order.last, st));
   c->launched = true;
   c->synced = false;
   c->copies_pending = false;
