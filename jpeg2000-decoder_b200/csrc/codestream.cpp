@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <cstring>
 
 namespace j2k {
@@ -137,6 +138,18 @@ struct TagTree {
   }
 };
 
+// A block's coded pieces (one per contributing layer and segment) and codeword-segment
+// lengths are singly linked lists in per-tile arrays, so blocks allocate nothing.
+struct Piece {
+  const uint8_t *p;
+  uint32_t len;
+  int32_t next;
+};
+struct SegLen {
+  uint32_t len;
+  int32_t next;
+};
+
 struct CbState {
   int x0, y0, w, h;        // band coordinates relative to the band origin
   int passes = 0;          // passes signalled so far
@@ -144,8 +157,9 @@ struct CbState {
   int lblock = 3;
   int missing = 0;
   bool included = false;
-  std::vector<std::pair<const uint8_t *, uint32_t>> pieces;
-  std::vector<uint32_t> seglen;  // per codeword segment
+  int32_t piece_head = -1, piece_tail = -1;  // into the tile's Piece array
+  int32_t seg_head = -1, seg_tail = -1;      // into the tile's SegLen array
+  uint32_t nseg = 0;                         // codeword segments
 };
 
 struct BandState {
@@ -176,6 +190,44 @@ struct TCState {
   std::vector<ResState> res;
   uint64_t coef_off = 0;
 };
+
+// Copies the coded bytes of a tile's blocks (piece lists into the codestream) to their
+// places in `dst`; jobs = (block, byte offset), in offset order.  A tile of at least 4 MB is
+// split by bytes across up to 8 threads.
+void copy_pieces(uint8_t *dst, const std::vector<Piece> &pieces, const std::vector<std::pair<const CbState *, size_t>> &jobs,
+                 size_t total) {
+  auto run = [&](size_t lo, size_t hi) {
+    for (size_t j = lo; j < hi; ++j) {
+      uint8_t *o = dst + jobs[j].second;
+      for (int32_t i = jobs[j].first->piece_head; i >= 0; i = pieces[i].next) {
+        std::memcpy(o, pieces[i].p, pieces[i].len);
+        o += pieces[i].len;
+      }
+    }
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = total >= (size_t(4) << 20) ? std::min<size_t>(8, hw) : 1;
+  if (nt <= 1 || jobs.size() < 2 * nt) {
+    run(0, jobs.size());
+    return;
+  }
+  std::vector<size_t> cut(nt + 1, jobs.size());
+  cut[0] = 0;
+  for (size_t k = 1, j = 0; k < nt; ++k) {
+    while (j < jobs.size() && jobs[j].second < total * k / nt) ++j;
+    cut[k] = j;
+  }
+  std::vector<std::thread> th;
+  for (size_t i = 1; i < nt; ++i) {
+    try {
+      th.emplace_back(run, cut[i], cut[i + 1]);
+    } catch (...) {  // no thread: copy this range here
+      run(cut[i], cut[i + 1]);
+    }
+  }
+  run(cut[0], cut[1]);
+  for (auto &x : th) x.join();
+}
 
 bool seg_starts(int style, int j) {
   int type = (j == 0) ? 2 : (j - 1) % 3;
@@ -490,12 +542,12 @@ namespace {
 constexpr size_t kPoolMinBytes = size_t(1) << 20, kPoolMaxBytes = size_t(512) << 20;
 constexpr size_t kPoolMaxBuffers = 8;
 std::mutex g_pool_mu;
-std::vector<std::vector<uint8_t>> g_pool;
+std::vector<ByteBuffer> g_pool;
 size_t g_pool_bytes = 0;
 }  // namespace
 
-std::vector<uint8_t> take_plan_bytes(size_t capacity) {
-  std::vector<uint8_t> v;
+ByteBuffer take_plan_bytes(size_t capacity) {
+  ByteBuffer v;
   if (capacity >= kPoolMinBytes) {
     std::lock_guard<std::mutex> lk(g_pool_mu);
     size_t best = g_pool.size();
@@ -515,7 +567,7 @@ std::vector<uint8_t> take_plan_bytes(size_t capacity) {
   return v;
 }
 
-void give_plan_bytes(std::vector<uint8_t> &&bytes) {
+void give_plan_bytes(ByteBuffer &&bytes) {
   if (bytes.capacity() < kPoolMinBytes) return;
   std::lock_guard<std::mutex> lk(g_pool_mu);
   if (g_pool.size() >= kPoolMaxBuffers || g_pool_bytes + bytes.capacity() > kPoolMaxBytes) return;
@@ -648,6 +700,7 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     int tx0 = std::max(TH.tx0 + tx * TH.tile_w, TH.x0), ty0 = std::max(TH.ty0 + ty * TH.tile_h, TH.y0);
     int tx1 = std::min(TH.tx0 + (tx + 1) * TH.tile_w, TH.width), ty1 = std::min(TH.ty0 + (ty + 1) * TH.tile_h, TH.height);
     std::vector<TCState> tcs(TH.ncomp);
+    size_t tile_blocks = 0;
     for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       TC.comp = c;
@@ -742,11 +795,9 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
                   cb.y0 = gy0 - B.y0;
                   cb.w = gx1 - gx0;
                   cb.h = gy1 - gy0;
-                  // one piece per contributing layer, usually one segment per layer
-                  cb.pieces.reserve(std::min(TH.layers, 16));
-                  cb.seglen.reserve(std::min(TH.layers, 16));
                   B.prec_cbs[p].push_back((int)B.cbs.size());
-                  B.cbs.push_back(std::move(cb));
+                  B.cbs.push_back(cb);
+                  ++tile_blocks;
                 }
             }
         }
@@ -754,6 +805,10 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     }
 
     // ---- packets
+    std::vector<Piece> pieces;  // the tile's coded pieces, linked per block
+    std::vector<SegLen> segs;   // the tile's codeword-segment lengths, linked per block
+    pieces.reserve(tile_blocks * (size_t)std::min(TH.layers, 8));
+    segs.reserve(tile_blocks * (size_t)std::min(TH.layers, 8));
     const uint8_t *cur = nullptr, *end = nullptr;
     size_t part = 0;
     auto next_part = [&]() -> bool {
@@ -865,10 +920,24 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             stream_end = true;
           }
           if (keep) {
-            if (L) cb.pieces.push_back({cur, L});
-            bool newseg = (i > 0) || ct.first_seg_new;
-            if (newseg || cb.seglen.empty()) cb.seglen.push_back(L);
-            else cb.seglen.back() += L;
+            if (L) {
+              const int32_t at = (int32_t)pieces.size();
+              pieces.push_back({cur, L, -1});
+              if (cb.piece_tail >= 0) pieces[cb.piece_tail].next = at;
+              else cb.piece_head = at;
+              cb.piece_tail = at;
+            }
+            const bool newseg = (i > 0) || ct.first_seg_new;
+            if (newseg || cb.nseg == 0) {
+              const int32_t at = (int32_t)segs.size();
+              segs.push_back({L, -1});
+              if (cb.seg_tail >= 0) segs[cb.seg_tail].next = at;
+              else cb.seg_head = at;
+              cb.seg_tail = at;
+              cb.nseg++;
+            } else {
+              segs[cb.seg_tail].len += L;
+            }
           }
           cur += L;
         }
@@ -961,7 +1030,10 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     }
     if (rc != PARSE_OK) return rc;
 
-    // ---- emit plan entries for this tile
+    // ---- emit plan entries for this tile: the block table first, then the coded bytes
+    const size_t tile_base = P.bytes.size();
+    size_t tile_bytes = 0;
+    std::vector<std::pair<const CbState *, size_t>> copies;  // block, byte offset in the tile
     for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       if ((opt.ignore_components >> c) & 1) continue;
@@ -998,22 +1070,23 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             d.gain = B.gain;
             d.out_stride = (uint32_t)tc.w;
             d.out_off = tc.coef_off + (uint64_t)(B.off_y + cb.y0) * tc.w + (B.off_x + cb.x0);
-            d.data_off = (uint32_t)P.bytes.size();
+            d.data_off = (uint32_t)(tile_base + tile_bytes);
             uint32_t total = 0;
-            for (auto &pc : cb.pieces) {
-              P.bytes.insert(P.bytes.end(), pc.first, pc.first + pc.second);
-              total += pc.second;
-            }
+            for (int32_t i = cb.piece_head; i >= 0; i = pieces[i].next) total += pieces[i].len;
+            if (total) copies.push_back({&cb, tile_bytes});
+            tile_bytes += total;
             d.data_len = total;
             d.seg_off = (uint32_t)P.seglens.size();
-            d.nseg = (uint8_t)std::min<size_t>(cb.seglen.size(), 255);
-            for (uint32_t s : cb.seglen) P.seglens.push_back(s);
+            d.nseg = (uint8_t)std::min<uint32_t>(cb.nseg, 255);
+            for (int32_t i = cb.seg_head; i >= 0; i = segs[i].next) P.seglens.push_back(segs[i].len);
             if (cb.kept == 0) d.nseg = 0;
             P.cblks.push_back(d);
           }
         }
       }
     }
+    P.bytes.resize(tile_base + tile_bytes);
+    copy_pieces(P.bytes.data() + tile_base, pieces, copies, tile_bytes);
   }
   if (P.bytes.size() > 0xFFFFFFF0ull) return PARSE_ERR_UNSUPPORTED;
 

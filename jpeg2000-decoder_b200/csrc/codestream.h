@@ -14,7 +14,11 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
+#include <new>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "plan.h"
@@ -35,6 +39,28 @@ struct DecodeOptions {
   int max_layers = 0;        /* 0: all layers */
   unsigned ignore_components = 0; /* bit c set: component c is not decoded */
 };
+
+/* std::allocator whose value-initialisation leaves the element unset: a plan's byte buffer
+ * is resized and then filled by the Tier-2 copy, so zeroing it first is wasted work. */
+template <class T>
+struct NoInitAllocator : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAllocator<U>;
+  };
+  NoInitAllocator() = default;
+  template <class U>
+  NoInitAllocator(const NoInitAllocator<U> &) noexcept {}
+  template <class U>
+  void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new ((void *)p) U;
+  }
+  template <class U, class... A>
+  void construct(U *p, A &&...a) {
+    ::new ((void *)p) U(std::forward<A>(a)...);
+  }
+};
+using ByteBuffer = std::vector<uint8_t, NoInitAllocator<uint8_t>>;
 
 /* One progression volume of a POC marker (T.800 A.6.6): layers [0, lye), resolutions
  * [rs, re), components [cs, ce) in progression order `prog`. */
@@ -77,7 +103,7 @@ struct ImagePlan {
   j2k_image_info info{};
   std::vector<j2k_cblk> cblks;
   std::vector<uint32_t> seglens;
-  std::vector<uint8_t> bytes;         /* Tier-1 bytes, block after block */
+  ByteBuffer bytes;                   /* Tier-1 bytes, block after block */
   std::vector<j2k_tilecomp> tilecomps;
   int out_w = 0, out_h = 0;           /* output size after discard_levels */
   int discard = 0;
@@ -89,8 +115,8 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &hdr);
  * its first write, about a quarter of the Tier-2 time).  take_plan_bytes returns an empty
  * buffer with at least `capacity` bytes reserved; give_plan_bytes hands a plan's buffer back
  * (kept while the pool holds fewer than 8 buffers and under 512 MB). */
-std::vector<uint8_t> take_plan_bytes(size_t capacity);
-void give_plan_bytes(std::vector<uint8_t> &&bytes);
+ByteBuffer take_plan_bytes(size_t capacity);
+void give_plan_bytes(ByteBuffer &&bytes);
 int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImagePlan &plan);
 const char *status_string(int status);
 

@@ -769,7 +769,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::memcpy(H + o_ftk + ftasks[0].size() * sizeof(OutTask), ftasks[1].data(), ftasks[1].size() * sizeof(OutTask));
   {
     // coded bytes of every image, copied by a few threads when there are many
-    std::vector<std::pair<size_t, const std::vector<uint8_t> *>> parts;
+    std::vector<std::pair<size_t, const j2k::ByteBuffer *>> parts;
     size_t off = o_byt;
     for (auto &im : c->imgs) {
       parts.push_back({off, &im.plan->p.bytes});

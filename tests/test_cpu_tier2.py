@@ -111,3 +111,33 @@ def test_cinema_profile_poc_and_tile_parts(pkg):
     rgb = _oracle_rgb(cs, 1080, 2048).astype(int)
     ref = np.asarray(Image.open(io.BytesIO(cs)).convert("RGB")).astype(int)
     assert np.abs(rgb - ref).max() <= 1
+
+
+def test_large_plans_threaded_copy_and_concurrency(pkg):
+    """A plan of more than 4 MB of coded bytes copies them on several threads and recycles
+    its buffer; plans made concurrently from several threads are identical, and the picture
+    decodes to its source."""
+    import ctypes
+    import hashlib
+    from concurrent.futures import ThreadPoolExecutor
+    from jpeg2000_decoder_b200 import native, synth
+    img = synth.fractal_rgb(7, 768, 1536, bitdepth=12)
+    cs = native.encode(img, 12, reversible=1, levels=5, cbw_exp=5, cbh_exp=5, num_layers=4,
+                       layer_bpp=[1, 3, 6, 0], progression=2, mode=3)
+    assert len(cs) > (4 << 20)
+
+    def digest(_):
+        p = native.Plan(cs)
+        h = hashlib.sha1(ctypes.string_at(native.lib().j2k_plan_bytes(p.h), p.info.coded_bytes))
+        h.update(bytes(p.cblks()))
+        h.update(ctypes.string_at(native.lib().j2k_plan_seglens(p.h), 4 * p.info.num_segs))
+        return h.hexdigest()
+
+    with ThreadPoolExecutor(8) as ex:
+        digests = list(ex.map(digest, range(16)))
+    assert len(set(digests)) == 1
+    plan = native.Plan(cs)
+    rc, out, _ = oracle_util.oracle_decode(plan, native.FMT_48BITS_RGB)
+    assert rc == 0
+    rgb = out.view(np.uint16).reshape(768, 1536, 3)[:, :, ::-1].transpose(2, 0, 1) >> 4
+    assert np.array_equal(rgb, img)
