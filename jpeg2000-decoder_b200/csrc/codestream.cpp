@@ -523,6 +523,8 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   if (!have_siz || !have_cod || !have_qcd) return PARSE_ERR_MARKER;
   if (H.width <= H.x0 || H.height <= H.y0 || H.tile_w <= 0 || H.tile_h <= 0) return PARSE_ERR_INVALID;
   if (H.x0 || H.y0 || H.tx0 || H.ty0) return PARSE_ERR_UNSUPPORTED;
+  // tile indices are 16-bit, 65535 excluded (T.800 A.4.2)
+  if ((int64_t)H.ntx() * H.nty() > 65535) return PARSE_ERR_INVALID;
   for (int c = 0; c < H.ncomp; ++c) {
     if (H.sub_x[c] != 1 || H.sub_y[c] != 1) return PARSE_ERR_UNSUPPORTED;
     if (H.depth[c] > 16 || H.depth[c] != H.depth[0]) return PARSE_ERR_UNSUPPORTED;
@@ -975,20 +977,22 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     std::vector<PocEntry> vols = TH.poc;
     if (vols.empty()) vols.push_back({0, 0, TH.layers, maxL + 1, TH.ncomp, TH.progression});
     int rc = PARSE_OK;
+    // a tile whose data (or packed headers) ran out has no packet left to read
+    auto go = [&]() { return rc == PARSE_OK && !stream_end; };
     for (const PocEntry &v : vols) {
       const int lye = std::min(v.lye, TH.layers), re = std::min(v.re, maxL + 1), ce = std::min(v.ce, TH.ncomp);
       const int rs = v.rs, cs = v.cs;
       if (rs >= re || cs >= ce || lye <= 0) continue;
       if (v.prog == 0) {  // LRCP
-        for (int l = 0; l < lye && rc == PARSE_OK; ++l)
-          for (int r = rs; r < re && rc == PARSE_OK; ++r)
-            for (int c = cs; c < ce && rc == PARSE_OK; ++c)
-              for (int p = 0; p < nprec(r, c) && rc == PARSE_OK; ++p) rc = visit(l, r, c, p);
+        for (int l = 0; l < lye && go(); ++l)
+          for (int r = rs; r < re && go(); ++r)
+            for (int c = cs; c < ce && go(); ++c)
+              for (int p = 0; p < nprec(r, c) && go(); ++p) rc = visit(l, r, c, p);
       } else if (v.prog == 1) {  // RLCP
-        for (int r = rs; r < re && rc == PARSE_OK; ++r)
-          for (int l = 0; l < lye && rc == PARSE_OK; ++l)
-            for (int c = cs; c < ce && rc == PARSE_OK; ++c)
-              for (int p = 0; p < nprec(r, c) && rc == PARSE_OK; ++p) rc = visit(l, r, c, p);
+        for (int r = rs; r < re && go(); ++r)
+          for (int l = 0; l < lye && go(); ++l)
+            for (int c = cs; c < ce && go(); ++c)
+              for (int p = 0; p < nprec(r, c) && go(); ++p) rc = visit(l, r, c, p);
       } else {  // RPCL, PCRL, CPRL
         pv.clear();
         for (int c = cs; c < ce; ++c) {
@@ -1024,9 +1028,9 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
           return a.r < b.r;
         });
         for (const PrecinctVisit &q : pv)
-          for (int l = 0; l < lye && rc == PARSE_OK; ++l) rc = visit(l, q.r, q.c, q.p);
+          for (int l = 0; l < lye && go(); ++l) rc = visit(l, q.r, q.c, q.p);
       }
-      if (rc != PARSE_OK) break;
+      if (!go()) break;
     }
     if (rc != PARSE_OK) return rc;
 

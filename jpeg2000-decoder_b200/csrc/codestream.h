@@ -93,8 +93,8 @@ struct StreamHeader {
   bool has_ppm = false;
   size_t header_len = 0;    /* bytes up to the first SOT */
   size_t cs_offset = 0;     /* offset of SOC inside the input (JP2 wrapper) */
-  int ntx() const { return (width - tx0 + tile_w - 1) / tile_w; }
-  int nty() const { return (height - ty0 + tile_h - 1) / tile_h; }
+  int ntx() const { return (int)(((int64_t)width - tx0 + tile_w - 1) / tile_w); }
+  int nty() const { return (int)(((int64_t)height - ty0 + tile_h - 1) / tile_h); }
 };
 
 /* The full host-side plan of one image. */

@@ -18,7 +18,18 @@ extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels
   opt.discard_levels = discard_levels < 0 ? 0 : discard_levels;
   opt.max_layers = max_layers;
   opt.ignore_components = ignore_components;
-  int rc = j2k::build_plan(cs, len, opt, p->p);
+  // the stream's sizes drive host allocations: an oversized (or corrupt but well-formed)
+  // header fails here with an error code instead of an exception through the C ABI
+  int rc;
+  try {
+    rc = j2k::build_plan(cs, len, opt, p->p);
+  } catch (const std::bad_alloc &) {
+    delete p;
+    return J2K_ERR_NOMEM;
+  } catch (...) {
+    delete p;
+    return J2K_ERR_PARSE;
+  }
   if (rc != j2k::PARSE_OK) {
     delete p;
     return rc == j2k::PARSE_ERR_UNSUPPORTED ? J2K_ERR_UNSUPPORTED : J2K_ERR_PARSE;

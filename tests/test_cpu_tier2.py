@@ -141,3 +141,47 @@ def test_large_plans_threaded_copy_and_concurrency(pkg):
     assert rc == 0
     rgb = out.view(np.uint16).reshape(768, 1536, 3)[:, :, ::-1].transpose(2, 0, 1) >> 4
     assert np.array_equal(rgb, img)
+
+
+def test_mutated_streams_are_planned_or_refused(pkg):
+    """Seeded corruptions (bytes flipped in the headers or anywhere, truncations, runs
+    inserted or deleted) of the Tier-2 variant streams: every call returns a plan or an
+    error code, never an exception through the C ABI or a crash, and a tenth of the plans
+    also go through the oracle's decode."""
+    import random
+    from jpeg2000_decoder_b200 import native
+    seeds = []
+    for name in sorted(os.listdir(FIX)):
+        if name.endswith(".j2k"):
+            with open(os.path.join(FIX, name), "rb") as f:
+                seeds.append(f.read())
+    seeds += [ts.encode_case(kw) for _, kw, _ in ts.marker_cases()]
+    seeds += [cs for _, cs in ts.splice_cases()]
+    rng = random.Random(1234)
+    planned = refused = 0
+    for _ in range(1500):
+        cs = bytearray(rng.choice(seeds))
+        kind = rng.randrange(4)
+        if kind == 0:
+            for _ in range(rng.randint(1, 4)):
+                cs[rng.randrange(min(len(cs), 400))] = rng.randrange(256)
+        elif kind == 1:
+            for _ in range(rng.randint(1, 16)):
+                cs[rng.randrange(len(cs))] = rng.randrange(256)
+        elif kind == 2:
+            cs = cs[: rng.randrange(2, len(cs))]
+        else:
+            j = rng.randrange(len(cs))
+            if rng.random() < 0.5:
+                cs[j:j] = bytes(rng.randrange(256) for _ in range(rng.randint(1, 8)))
+            else:
+                del cs[j:j + rng.randint(1, 8)]
+        try:
+            plan = native.Plan(bytes(cs))
+        except native.J2kError:
+            refused += 1
+            continue
+        planned += 1
+        if rng.random() < 0.1 and plan.info.coef_elems < (1 << 24):
+            oracle_util.oracle_decode(plan, native.FMT_NONE)
+    assert planned > 0 and refused > 0
