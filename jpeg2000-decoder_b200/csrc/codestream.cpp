@@ -720,11 +720,10 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
         R.y0 = ceil_div_pow2(TC.y0, nb);
         R.x1 = ceil_div_pow2(TC.x1, nb);
         R.y1 = ceil_div_pow2(TC.y1, nb);
-        // the device DWT assumes even origins at every resolution (the reference's HDWT
-        // ignores xParity as well, bmi_cpu_dwt_decoder.cpp:2609)
-        if ((R.x0 & 1) || (R.y0 & 1)) {
-          if (r < L) return PARSE_ERR_UNSUPPORTED;
-        }
+        // the device DWT synthesises every resolution r >= 1 with its first sample low-pass,
+        // i.e. from an even origin (the reference's HDWT ignores xParity as well,
+        // bmi_cpu_dwt_decoder.cpp:2609); the coarsest LL band (r = 0) is never synthesised
+        if (r > 0 && ((R.x0 & 1) || (R.y0 & 1))) return PARSE_ERR_UNSUPPORTED;
         int ppx = TH.ppx[c][r], ppy = TH.ppy[c][r];
         if (R.x1 > R.x0 && R.y1 > R.y0) {
           R.npx = ((R.x1 + (1 << ppx) - 1) >> ppx) - (R.x0 >> ppx);

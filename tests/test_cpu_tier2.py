@@ -185,3 +185,16 @@ def test_mutated_streams_are_planned_or_refused(pkg):
         if rng.random() < 0.1 and plan.info.coef_elems < (1 << 24):
             oracle_util.oracle_decode(plan, native.FMT_NONE)
     assert planned > 0 and refused > 0
+
+
+def test_randomized_encoder_roundtrips(pkg):
+    """120 seeded lossless configurations (levels, block sizes, layers, mode switches,
+    progressions, tilings, SOP/EPH, PPM/PPT, tile-parts, POC) decode to their sources."""
+    from jpeg2000_decoder_b200 import native
+    for i, (kw, depth, h, w) in enumerate(ts.random_cases(2024, 120)):
+        img, cs = ts.random_case_stream(2024, i, kw, depth, h, w)
+        plan = native.Plan(cs)
+        fmt = native.FMT_24BITS_RGB if depth == 8 else native.FMT_48BITS_RGB
+        rc, out, _ = oracle_util.oracle_decode(plan, fmt)
+        assert rc == 0, (i, kw)
+        assert np.array_equal(ts.rgb_of(out, depth, h, w), img), (i, kw)

@@ -397,3 +397,16 @@ def test_tier2_variants_bit_exact(gpu_ctx):
         if src is not None:
             I = plan.info
             assert np.array_equal(ts.as_rgb(out, I.height, I.width), src), name
+
+
+def test_randomized_encoder_configurations_bit_exact(gpu_ctx):
+    """Seeded lossless configurations (tilings whose coarsest LL band starts on an odd
+    coordinate included) decode on the device exactly as the oracle decodes them and
+    reproduce their sources."""
+    from jpeg2000_decoder_b200 import native
+    import tier2_streams as ts
+    for i, (kw, depth, h, w) in enumerate(ts.random_cases(2025, 24)):
+        img, cs = ts.random_case_stream(2025, i, kw, depth, h, w)
+        fmt = native.FMT_24BITS_RGB if depth == 8 else native.FMT_48BITS_RGB
+        out, plan = _decode_check(gpu_ctx, cs, fmt)
+        assert np.array_equal(ts.rgb_of(out, depth, h, w), img), (i, kw)

@@ -125,3 +125,58 @@ def transform_mismatch_stream():
 def as_rgb(out, h=H, w=W):
     """24-bit output (B, G, R byte order) as (3, h, w) uint16 planes."""
     return np.ascontiguousarray(out.reshape(h, w, 3)[:, :, ::-1].transpose(2, 0, 1)).astype(np.uint16)
+
+
+def random_cases(seed, n):
+    """(keywords, bit depth, height, width) of `n` seeded lossless encoder configurations:
+    levels 0-4, code-block sizes 4..64, 1-5 layers, mode switches, all progressions, tiles
+    of any multiple of 2^levels (the coarsest LL band may start on an odd coordinate),
+    SOP / EPH, PPM or PPT, tile-parts (interleaved or not) and POC volumes covering every
+    packet."""
+    import random
+    from jpeg2000_decoder_b200 import native
+    rng = random.Random(seed)
+    out = []
+    for _ in range(n):
+        L = rng.randint(0, 4)
+        h, w = rng.randint(17, 120), rng.randint(17, 150)
+        depth = rng.choice([8, 12])
+        NL = rng.randint(1, 5)
+        bpp = sorted(rng.uniform(0.3, 6) for _ in range(NL - 1)) + [0]
+        kw = dict(reversible=1, levels=L, num_layers=NL, layer_bpp=bpp, cbw_exp=rng.randint(2, 6),
+                  cbh_exp=rng.randint(2, 6), mode=rng.choice([0, 1, 2, 3, 4, 0x20, 0x33, 0x37]),
+                  progression=rng.randrange(5))
+        kw["cbh_exp"] = min(kw["cbh_exp"], 12 - kw["cbw_exp"])
+        if rng.random() < 0.6:
+            t = 1 << L
+            kw["tile_w"] = t * rng.randint(max(1, 16 // t), max(2, 64 // t))
+            kw["tile_h"] = t * rng.randint(max(1, 16 // t), max(2, 64 // t))
+        m = (native.ENC_SOP if rng.random() < 0.4 else 0) | (native.ENC_EPH if rng.random() < 0.4 else 0)
+        r = rng.random()
+        m |= native.ENC_PPM if r < 0.25 else (native.ENC_PPT if r < 0.5 else 0)
+        kw["markers"] = m
+        if rng.random() < 0.5:
+            kw["tile_parts"] = rng.randint(2, 5)
+            kw["interleave_tile_parts"] = rng.randrange(2)
+        if rng.random() < 0.4:
+            vols = [(0, 0, rng.randint(1, NL), rng.randint(1, L + 1), rng.randint(1, 3), rng.randrange(5)),
+                    (0, 0, NL, L + 1, 3, rng.randrange(5))]
+            if rng.random() < 0.5:
+                vols.insert(1, (rng.randint(0, L), 0, NL, L + 1, 3, rng.randrange(5)))
+            kw["poc"] = vols
+            kw["poc_in_tiles"] = rng.randrange(2)
+        out.append((kw, depth, h, w))
+    return out
+
+
+def random_case_stream(seed, i, kw, depth, h, w):
+    from jpeg2000_decoder_b200 import native, synth
+    img = synth.fractal_rgb(seed * 1000 + i, h, w, bitdepth=depth)
+    return img, native.encode(img, depth, **kw)
+
+
+def rgb_of(out, depth, h, w):
+    """Packed 24-bit (8-bit pictures) or 48-bit (12-bit pictures) output as (3, h, w)."""
+    if depth == 8:
+        return out.reshape(h, w, 3)[:, :, ::-1].transpose(2, 0, 1).astype(np.uint16)
+    return out.view(np.uint16).reshape(h, w, 3)[:, :, ::-1].transpose(2, 0, 1) >> 4
