@@ -62,12 +62,12 @@ int fmt_bytes(int fmt) {
 
 void fill_props(const j2k::StreamHeader &H, int discard, CodeStreamProperties &P, OutputFormat fmt) {
   std::memset(&P, 0, sizeof(P));
-  P.mSize.x = (short)H.width;
-  P.mSize.y = (short)H.height;
-  P.mOutputSize.x = (short)((H.width + (1 << discard) - 1) >> discard);
-  P.mOutputSize.y = (short)((H.height + (1 << discard) - 1) >> discard);
-  P.mThumbOutputSize.x = (short)((H.width + (1 << H.levels[0]) - 1) >> H.levels[0]);
-  P.mThumbOutputSize.y = (short)((H.height + (1 << H.levels[0]) - 1) >> H.levels[0]);
+  P.mSize.x = (short)H.image_w();
+  P.mSize.y = (short)H.image_h();
+  P.mOutputSize.x = (short)H.out_w(discard);
+  P.mOutputSize.y = (short)H.out_h(discard);
+  P.mThumbOutputSize.x = (short)H.out_w(H.levels[0]);
+  P.mThumbOutputSize.y = (short)H.out_h(H.levels[0]);
   P.mOutputFormat = fmt;
   P.mCodeBlockSize.x = (short)(1 << H.cbw_exp[0]);
   P.mCodeBlockSize.y = (short)(1 << H.cbh_exp[0]);

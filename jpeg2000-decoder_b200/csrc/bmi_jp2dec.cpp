@@ -88,8 +88,8 @@ extern "C" int BMI_dec_info(stru_dec_param *p, int thread_num) {
   if (!p || !p->input || p->in_size < 2) return -1;
   j2k::StreamHeader H;
   if (j2k::parse_header((const uint8_t *)p->input, p->in_size, H) != j2k::PARSE_OK) return -1;
-  p->width = H.width;
-  p->height = H.height;
+  p->width = H.image_w();
+  p->height = H.image_h();
   p->bitdepth = H.depth[0];
   p->num_components = H.ncomp;
   p->format = H.ncomp;
@@ -110,7 +110,7 @@ extern "C" int BMI_dec_info(stru_dec_param *p, int thread_num) {
   p->guard_bit = H.guard[0];
   for (int i = 0; i <= 3 * MAX_DWT_LEVEL; ++i) p->quant_step[i] = H.steps[0][i];
   // pool 0: host Tier-2 state; pool 1: one decoded picture (4 bytes per sample)
-  const size_t samples = (size_t)H.width * H.height * H.ncomp;
+  const size_t samples = (size_t)H.image_w() * H.image_h() * H.ncomp;
   p->pool_size[0] = (int)std::min<size_t>(0x7FFFFFFF, p->in_size + samples / 16 + 4096);
   p->pool_size[1] = (int)std::min<size_t>(0x7FFFFFFF, samples * 4);
   p->size_opt = 0;

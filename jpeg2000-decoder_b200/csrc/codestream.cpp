@@ -521,8 +521,12 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
     if (rc != PARSE_OK) return rc;
   }
   if (!have_siz || !have_cod || !have_qcd) return PARSE_ERR_MARKER;
+  if (H.x0 < 0 || H.y0 < 0 || H.tx0 < 0 || H.ty0 < 0) return PARSE_ERR_INVALID;  // above 2^31
   if (H.width <= H.x0 || H.height <= H.y0 || H.tile_w <= 0 || H.tile_h <= 0) return PARSE_ERR_INVALID;
-  if (H.x0 || H.y0 || H.tx0 || H.ty0) return PARSE_ERR_UNSUPPORTED;
+  // the tile grid starts at or above-left of the image origin and its first tile meets the
+  // image (T.800 A.5.1)
+  if (H.tx0 > H.x0 || H.ty0 > H.y0 || (int64_t)H.tx0 + H.tile_w <= H.x0 || (int64_t)H.ty0 + H.tile_h <= H.y0)
+    return PARSE_ERR_INVALID;
   // tile indices are 16-bit, 65535 excluded (T.800 A.4.2)
   if ((int64_t)H.ntx() * H.nty() > 65535) return PARSE_ERR_INVALID;
   for (int c = 0; c < H.ncomp; ++c) {
@@ -693,14 +697,18 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
 
   // ---- geometry and Tier-2 per tile
   uint64_t coef_total = 0;
-  P.out_w = ceil_div_pow2(H.width, discard);
-  P.out_h = ceil_div_pow2(H.height, discard);
+  P.out_w = H.out_w(discard);
+  P.out_h = H.out_h(discard);
+  // tile-components are placed relative to the image origin at the output resolution
+  const int ox = ceil_div_pow2(H.x0, discard), oy = ceil_div_pow2(H.y0, discard);
   for (int t = 0; t < ntiles; ++t) {
     const StreamHeader &TH = tile_header(t);
     const int maxlayers = opt.max_layers > 0 ? std::min(opt.max_layers, TH.layers) : TH.layers;
     int tx = t % ntx, ty = t / ntx;
-    int tx0 = std::max(TH.tx0 + tx * TH.tile_w, TH.x0), ty0 = std::max(TH.ty0 + ty * TH.tile_h, TH.y0);
-    int tx1 = std::min(TH.tx0 + (tx + 1) * TH.tile_w, TH.width), ty1 = std::min(TH.ty0 + (ty + 1) * TH.tile_h, TH.height);
+    const int tx0 = (int)std::max<int64_t>(TH.tx0 + (int64_t)tx * TH.tile_w, TH.x0);
+    const int ty0 = (int)std::max<int64_t>(TH.ty0 + (int64_t)ty * TH.tile_h, TH.y0);
+    const int tx1 = (int)std::min<int64_t>(TH.tx0 + (int64_t)(tx + 1) * TH.tile_w, TH.width);
+    const int ty1 = (int)std::min<int64_t>(TH.ty0 + (int64_t)(ty + 1) * TH.tile_h, TH.height);
     std::vector<TCState> tcs(TH.ncomp);
     size_t tile_blocks = 0;
     for (int c = 0; c < TH.ncomp; ++c) {
@@ -1047,8 +1055,8 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       tc.tile = t;
       tc.levels = keep;
       const ResState &Rtop = TC.res[keep];
-      tc.x0 = Rtop.x0;
-      tc.y0 = Rtop.y0;
+      tc.x0 = Rtop.x0 - ox;
+      tc.y0 = Rtop.y0 - oy;
       tc.w = Rtop.x1 - Rtop.x0;
       tc.h = Rtop.y1 - Rtop.y0;
       for (int r = 0; r <= keep; ++r) {

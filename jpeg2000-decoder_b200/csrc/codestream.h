@@ -93,6 +93,12 @@ struct StreamHeader {
   bool has_ppm = false;
   size_t header_len = 0;    /* bytes up to the first SOT */
   size_t cs_offset = 0;     /* offset of SOC inside the input (JP2 wrapper) */
+  /* picture size: the reference grid from the image origin (x0, y0) to (width, height) */
+  int image_w() const { return width - x0; }
+  int image_h() const { return height - y0; }
+  /* picture size at 1/2^d resolution (T.800 B.5: ceil(width / 2^d) - ceil(x0 / 2^d)) */
+  int out_w(int d) const { return (int)((((int64_t)width + (1LL << d) - 1) >> d) - (((int64_t)x0 + (1LL << d) - 1) >> d)); }
+  int out_h(int d) const { return (int)((((int64_t)height + (1LL << d) - 1) >> d) - (((int64_t)y0 + (1LL << d) - 1) >> d)); }
   int ntx() const { return (int)(((int64_t)width - tx0 + tile_w - 1) / tile_w); }
   int nty() const { return (int)(((int64_t)height - ty0 + tile_h - 1) / tile_h); }
 };

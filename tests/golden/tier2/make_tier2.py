@@ -2,10 +2,11 @@
 
 OpenJPEG (the copy inside Pillow, `PIL.features.version("jpg_2000")`) writes small
 codestreams that exercise what the project's own writer does not: several precincts per
-resolution under every progression order, precinct-limited code-block sizes, partial tiles
-and 9/7 quantisation with two guard bits.  The lossless ones must decode to the source
-picture; for the 9/7 one OpenJPEG's own decoded picture is stored as the expected output
-(floating-point 9/7 implementations differ by at most one level after rounding).
+resolution under every progression order, precinct-limited code-block sizes, partial tiles,
+image and tile-grid origins other than (0, 0), and 9/7 quantisation with two guard bits.
+The lossless ones must decode to the source picture; for the 9/7 one OpenJPEG's own
+decoded picture is stored as the expected output (floating-point 9/7 implementations
+differ by at most one level after rounding).
 
     python tests/golden/tier2/make_tier2.py
 """
@@ -51,6 +52,14 @@ def main():
         save(name, progression=prog, precinct_size=(16, 16), codeblock_size=(8, 8), num_resolutions=4,
              quality_layers=[30, 10, 0], quality_mode="rates", tile_size=(64, 48))
         manifest["streams"][name] = {"expect": "source", "progression": prog}
+    for name, kw in [("ojp_offset32x16_tileorigin16x8_lrcp.j2k",
+                      dict(offset=(32, 16), tile_offset=(16, 8), tile_size=(64, 48), num_resolutions=4)),
+                     ("ojp_offset48x24_tileorigin40x20_pcrl.j2k",
+                      dict(offset=(48, 24), tile_offset=(40, 20), tile_size=(32, 32), num_resolutions=3,
+                           progression="PCRL"))]:
+        save(name, precinct_size=(16, 16), codeblock_size=(8, 8), quality_layers=[30, 10, 0],
+             quality_mode="rates", **kw)
+        manifest["streams"][name] = {"expect": "source", "origin": list(kw["offset"])}
     name = "ojp_cprl_97_guard2.j2k"
     cs = save(name, progression="CPRL", precinct_size=(32, 32), codeblock_size=(16, 16), num_resolutions=4,
               quality_layers=[12, 4], quality_mode="rates", irreversible=True, tile_size=(64, 48))

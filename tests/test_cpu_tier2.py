@@ -198,3 +198,28 @@ def test_randomized_encoder_roundtrips(pkg):
         rc, out, _ = oracle_util.oracle_decode(plan, fmt)
         assert rc == 0, (i, kw)
         assert np.array_equal(ts.rgb_of(out, depth, h, w), img), (i, kw)
+
+
+def test_image_and_tile_origins(pkg):
+    """Image and tile-grid origins other than (0, 0): the picture is the grid from the image
+    origin, reduced resolutions have T.800's ceil(Xsiz / 2^d) - ceil(XOsiz / 2^d) columns, and
+    an origin that makes a synthesised resolution start on an odd coordinate is refused."""
+    from jpeg2000_decoder_b200 import native
+    with open(os.path.join(FIX, "ojp_offset32x16_tileorigin16x8_lrcp.j2k"), "rb") as f:
+        cs = f.read()
+    man = _manifest()
+    for d in (0, 1, 2, 3):
+        plan = native.Plan(cs, discard_levels=d)
+        W, H = man["width"] + 32, man["height"] + 16  # Xsiz, Ysiz
+        assert (plan.info.width, plan.info.height) == (-(-W // 2 ** d) - (-(-32 // 2 ** d)),
+                                                         -(-H // 2 ** d) - (-(-16 // 2 ** d)))
+        rc, _, _ = oracle_util.oracle_decode(plan, native.FMT_24BITS_RGB)
+        assert rc == 0
+    Image = pytest.importorskip("PIL.Image")
+    src = np.load(os.path.join(FIX, "expected.npz"))["source"]
+    f = io.BytesIO()
+    Image.fromarray(src, "RGB").save(f, "JPEG2000", no_jp2=True, offset=(33, 16), tile_offset=(16, 8),
+                                     tile_size=(64, 48), num_resolutions=4)
+    with pytest.raises(native.J2kError) as e:
+        native.Plan(f.getvalue())
+    assert e.value.code == native.J2K_ERR_UNSUPPORTED
