@@ -73,6 +73,12 @@ typedef struct j2k_plan j2k_plan;
  * `max_layers` 0 = all; bit c of `ignore_components` skips component c. */
 int j2k_plan_create(const uint8_t *codestream, size_t len, int discard_levels, int max_layers,
                     unsigned ignore_components, j2k_plan **out);
+/* The same with the Tier-2 of a multi-tile picture spread over `threads` host threads (tiles
+ * are independent; the plan is identical for any thread count).  The counterpart of the
+ * reference's worker-thread count (EnginConfig::mThreadNum, codec_base.h; BMI_dec_init's
+ * thread_num, bmi_jp2dec.h:82) for the part of the decode that stays on the host. */
+int j2k_plan_create_mt(const uint8_t *codestream, size_t len, int discard_levels, int max_layers,
+                       unsigned ignore_components, int threads, j2k_plan **out);
 void j2k_plan_destroy(j2k_plan *plan);
 int j2k_plan_info(const j2k_plan *plan, j2k_image_info *info);
 const j2k_cblk *j2k_plan_cblks(const j2k_plan *plan);

@@ -160,7 +160,8 @@ class GpuDecoder : public Decoder {
     const int discard = discard_of(H);
     fill_props(H, discard, s.props, s.cfg.mOutputFormat);
     j2k_plan *plan = nullptr;
-    int rc = j2k_plan_create(s.codestream.data(), s.codestream.size(), discard, 0, s.cfg.mIgnoreComponents, &plan);
+    int rc = j2k_plan_create_mt(s.codestream.data(), s.codestream.size(), discard, 0, s.cfg.mIgnoreComponents, tier2_threads(),
+                                &plan);
     if (rc != J2K_OK) {
       s.status = rc == J2K_ERR_UNSUPPORTED ? PARSE_ERROR_UNSUPPORTED_FORMAT : PARSE_ERROR;
       return h;
@@ -268,6 +269,10 @@ class GpuDecoder : public Decoder {
     void operator()(j2k_plan *p) const { j2k_plan_destroy(p); }
   };
 
+  // host threads for the Tier-2 of a multi-tile picture: the engine's worker-thread count
+  // (the reference's default of one thread when it is not set)
+  int tier2_threads() const { return cfg_.mThreadNum > 1 ? cfg_.mThreadNum : 1; }
+
   int discard_of(const j2k::StreamHeader &H) const {
     int top = job_.mDwtDecodeTopLevel;
     if (top < 0 || top >= H.levels[0]) return 0;
@@ -309,7 +314,8 @@ class GpuDecoder : public Decoder {
   bool decode_side(Slot &s, int discard, int fmt, std::vector<uint8_t> &out) {
     finish_pending();
     j2k_plan *p = nullptr;
-    if (j2k_plan_create(s.codestream.data(), s.codestream.size(), discard, 0, s.cfg.mIgnoreComponents, &p) != J2K_OK)
+    if (j2k_plan_create_mt(s.codestream.data(), s.codestream.size(), discard, 0, s.cfg.mIgnoreComponents, tier2_threads(),
+                           &p) != J2K_OK)
       return false;
     j2k_image_info I;
     j2k_plan_info(p, &I);
@@ -331,8 +337,8 @@ class GpuDecoder : public Decoder {
     auto redecode = [&]() {
       finish_pending();
       j2k_plan *p = nullptr;
-      if (j2k_plan_create(s.codestream.data(), s.codestream.size(), discard_of_slot(s), 0, s.cfg.mIgnoreComponents,
-                          &p) != J2K_OK)
+      if (j2k_plan_create_mt(s.codestream.data(), s.codestream.size(), discard_of_slot(s), 0, s.cfg.mIgnoreComponents,
+                             tier2_threads(), &p) != J2K_OK)
         return false;
       plan_.reset(p);
       if (j2k_gpu_batch_begin(ctx_) != J2K_OK || j2k_gpu_batch_add(ctx_, p, J2K_FMT_NONE, 0, &s.gpu_slot) != J2K_OK ||

@@ -18,6 +18,8 @@
 #include "codestream.h"
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -191,41 +193,40 @@ struct TCState {
   uint64_t coef_off = 0;
 };
 
-// Copies the coded bytes of a tile's blocks (piece lists into the codestream) to their
-// places in `dst`; jobs = (block, byte offset), in offset order.  A tile of at least 4 MB is
-// split by bytes across up to 8 threads.
-void copy_pieces(uint8_t *dst, const std::vector<Piece> &pieces, const std::vector<std::pair<const CbState *, size_t>> &jobs,
-                 size_t total) {
-  auto run = [&](size_t lo, size_t hi) {
-    for (size_t j = lo; j < hi; ++j) {
-      uint8_t *o = dst + jobs[j].second;
-      for (int32_t i = jobs[j].first->piece_head; i >= 0; i = pieces[i].next) {
-        std::memcpy(o, pieces[i].p, pieces[i].len);
-        o += pieces[i].len;
-      }
+// The coded bytes of a plan are the concatenation of spans (pointer into the codestream,
+// length), cut into chunks of about 1 MB; a plan of at least 4 MB copies its chunks on up
+// to 8 threads.
+struct CopyChunk {
+  uint8_t *dst;
+  const std::pair<const uint8_t *, uint32_t> *b, *e;
+};
+void copy_chunks(const std::vector<CopyChunk> &chunks, size_t total) {
+  auto run = [&](const CopyChunk &k) {
+    uint8_t *o = k.dst;
+    for (auto *sp = k.b; sp != k.e; ++sp) {
+      std::memcpy(o, sp->first, sp->second);
+      o += sp->second;
     }
   };
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t nt = total >= (size_t(4) << 20) ? std::min<size_t>(8, hw) : 1;
-  if (nt <= 1 || jobs.size() < 2 * nt) {
-    run(0, jobs.size());
+  const size_t nt = total >= (size_t(4) << 20) ? std::min<size_t>(std::min<size_t>(8, hw), chunks.size()) : 1;
+  if (nt <= 1) {
+    for (const CopyChunk &k : chunks) run(k);
     return;
   }
-  std::vector<size_t> cut(nt + 1, jobs.size());
-  cut[0] = 0;
-  for (size_t k = 1, j = 0; k < nt; ++k) {
-    while (j < jobs.size() && jobs[j].second < total * k / nt) ++j;
-    cut[k] = j;
-  }
+  std::atomic<size_t> next{0};
+  auto worker = [&]() {
+    for (size_t i; (i = next.fetch_add(1)) < chunks.size();) run(chunks[i]);
+  };
   std::vector<std::thread> th;
   for (size_t i = 1; i < nt; ++i) {
     try {
-      th.emplace_back(run, cut[i], cut[i + 1]);
-    } catch (...) {  // no thread: copy this range here
-      run(cut[i], cut[i + 1]);
+      th.emplace_back(worker);
+    } catch (...) {  // no thread: the others take its share
+      break;
     }
   }
-  run(cut[0], cut[1]);
+  worker();
   for (auto &x : th) x.join();
 }
 
@@ -695,13 +696,24 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
   if (discard < 0) discard = 0;
   P.discard = discard;
 
-  // ---- geometry and Tier-2 per tile
-  uint64_t coef_total = 0;
+  // ---- geometry and Tier-2 per tile.  Tiles are independent: each fills a TileOut with
+  // tile-relative offsets, on `opt.threads` host threads; the outputs are then merged in
+  // tile order, so the plan does not depend on the thread count.
+  struct TileOut {
+    std::vector<j2k_tilecomp> tcs;
+    std::vector<j2k_cblk> cblks;
+    std::vector<uint32_t> seglens;
+    std::vector<std::pair<const uint8_t *, uint32_t>> spans;  // coded bytes, block after block
+    uint64_t coef = 0;
+    size_t bytes = 0;
+  };
+  std::vector<TileOut> outs(ntiles);
   P.out_w = H.out_w(discard);
   P.out_h = H.out_h(discard);
   // tile-components are placed relative to the image origin at the output resolution
   const int ox = ceil_div_pow2(H.x0, discard), oy = ceil_div_pow2(H.y0, discard);
-  for (int t = 0; t < ntiles; ++t) {
+  auto process_tile = [&](int t, TileOut &out) -> int {
+    uint64_t coef_total = 0;
     const StreamHeader &TH = tile_header(t);
     const int maxlayers = opt.max_layers > 0 ? std::min(opt.max_layers, TH.layers) : TH.layers;
     int tx = t % ntx, ty = t / ntx;
@@ -1041,10 +1053,8 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     }
     if (rc != PARSE_OK) return rc;
 
-    // ---- emit plan entries for this tile: the block table first, then the coded bytes
-    const size_t tile_base = P.bytes.size();
+    // ---- emit plan entries for this tile (offsets relative to the tile)
     size_t tile_bytes = 0;
-    std::vector<std::pair<const CbState *, size_t>> copies;  // block, byte offset in the tile
     for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       if ((opt.ignore_components >> c) & 1) continue;
@@ -1065,7 +1075,7 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       }
       tc.coef_off = coef_total;
       coef_total += (uint64_t)tc.w * tc.h;
-      P.tilecomps.push_back(tc);
+      out.tcs.push_back(tc);
       for (int r = 0; r <= keep; ++r) {
         for (auto &B : TC.res[r].bands) {
           for (auto &cb : B.cbs) {
@@ -1081,25 +1091,108 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             d.gain = B.gain;
             d.out_stride = (uint32_t)tc.w;
             d.out_off = tc.coef_off + (uint64_t)(B.off_y + cb.y0) * tc.w + (B.off_x + cb.x0);
-            d.data_off = (uint32_t)(tile_base + tile_bytes);
+            d.data_off = (uint32_t)tile_bytes;
             uint32_t total = 0;
-            for (int32_t i = cb.piece_head; i >= 0; i = pieces[i].next) total += pieces[i].len;
-            if (total) copies.push_back({&cb, tile_bytes});
+            for (int32_t i = cb.piece_head; i >= 0; i = pieces[i].next) {
+              total += pieces[i].len;
+              out.spans.push_back({pieces[i].p, pieces[i].len});
+            }
             tile_bytes += total;
             d.data_len = total;
-            d.seg_off = (uint32_t)P.seglens.size();
+            d.seg_off = (uint32_t)out.seglens.size();
             d.nseg = (uint8_t)std::min<uint32_t>(cb.nseg, 255);
-            for (int32_t i = cb.seg_head; i >= 0; i = segs[i].next) P.seglens.push_back(segs[i].len);
+            for (int32_t i = cb.seg_head; i >= 0; i = segs[i].next) out.seglens.push_back(segs[i].len);
             if (cb.kept == 0) d.nseg = 0;
-            P.cblks.push_back(d);
+            out.cblks.push_back(d);
           }
         }
       }
     }
-    P.bytes.resize(tile_base + tile_bytes);
-    copy_pieces(P.bytes.data() + tile_base, pieces, copies, tile_bytes);
+    out.coef = coef_total;
+    out.bytes = tile_bytes;
+    return PARSE_OK;
+  };
+
+  // run the tiles; the error of the first failing tile in tile order is reported
+  std::vector<int> tile_rc(ntiles, PARSE_OK);
+  const int nthreads = std::max(1, std::min(opt.threads, ntiles));
+  if (nthreads <= 1) {
+    for (int t = 0; t < ntiles; ++t)
+      if ((tile_rc[t] = process_tile(t, outs[t])) != PARSE_OK) return tile_rc[t];
+  } else {
+    std::atomic<int> next{0};
+    std::mutex ex_mu;
+    std::exception_ptr ex;
+    auto worker = [&]() {
+      for (int t; (t = next.fetch_add(1)) < ntiles;) {
+        try {
+          tile_rc[t] = process_tile(t, outs[t]);
+        } catch (...) {  // rethrown on the calling thread
+          std::lock_guard<std::mutex> lk(ex_mu);
+          if (!ex) ex = std::current_exception();
+          tile_rc[t] = PARSE_ERR_INVALID;
+        }
+      }
+    };
+    std::vector<std::thread> th;
+    for (int i = 1; i < nthreads; ++i) {
+      try {
+        th.emplace_back(worker);
+      } catch (...) {
+        break;
+      }
+    }
+    worker();
+    for (auto &x : th) x.join();
+    if (ex) std::rethrow_exception(ex);
+    for (int t = 0; t < ntiles; ++t)
+      if (tile_rc[t] != PARSE_OK) return tile_rc[t];
   }
-  if (P.bytes.size() > 0xFFFFFFF0ull) return PARSE_ERR_UNSUPPORTED;
+
+  // ---- merge in tile order
+  size_t n_tcs = 0, n_cblks = 0, n_segs = 0, n_bytes = 0;
+  for (const TileOut &o : outs) {
+    n_tcs += o.tcs.size();
+    n_cblks += o.cblks.size();
+    n_segs += o.seglens.size();
+    n_bytes += o.bytes;
+  }
+  if (n_bytes > 0xFFFFFFF0ull || n_segs > 0xFFFFFFF0ull) return PARSE_ERR_UNSUPPORTED;
+  P.tilecomps.reserve(n_tcs);
+  P.cblks.reserve(n_cblks);
+  P.seglens.reserve(n_segs);
+  P.bytes.resize(n_bytes);
+  uint64_t coef_total = 0;
+  size_t byte_base = 0;
+  std::vector<CopyChunk> chunks;
+  for (TileOut &o : outs) {
+    const uint32_t seg_base = (uint32_t)P.seglens.size();
+    for (j2k_tilecomp tc : o.tcs) {
+      tc.coef_off += coef_total;
+      P.tilecomps.push_back(tc);
+    }
+    for (j2k_cblk d : o.cblks) {
+      d.out_off += coef_total;
+      d.data_off += (uint32_t)byte_base;
+      d.seg_off += seg_base;
+      P.cblks.push_back(d);
+    }
+    P.seglens.insert(P.seglens.end(), o.seglens.begin(), o.seglens.end());
+    // chunks of about 1 MB of this tile's spans
+    uint8_t *dst = P.bytes.data() + byte_base;
+    const auto *b = o.spans.data(), *e = o.spans.data() + o.spans.size();
+    while (b != e) {
+      const auto *k = b;
+      size_t n = 0;
+      while (k != e && n < (size_t(1) << 20)) n += (k++)->second;
+      chunks.push_back({dst, b, k});
+      dst += n;
+      b = k;
+    }
+    coef_total += o.coef;
+    byte_base += o.bytes;
+  }
+  copy_chunks(chunks, n_bytes);
 
   j2k_image_info &I = P.info;
   I.width = P.out_w;

@@ -38,6 +38,7 @@ struct DecodeOptions {
   int discard_levels = 0;    /* decode at 1/2^n resolution (reference mDwtDecodeTopLevel) */
   int max_layers = 0;        /* 0: all layers */
   unsigned ignore_components = 0; /* bit c set: component c is not decoded */
+  int threads = 1;           /* host threads for the Tier-2 of a multi-tile picture */
 };
 
 /* std::allocator whose value-initialisation leaves the element unset: a plan's byte buffer

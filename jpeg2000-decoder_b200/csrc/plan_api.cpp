@@ -8,8 +8,8 @@
 #include "../../include/j2k_gpu.h"
 #include "codestream.h"
 
-extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels, int max_layers,
-                               unsigned ignore_components, j2k_plan **out) {
+extern "C" int j2k_plan_create_mt(const uint8_t *cs, size_t len, int discard_levels, int max_layers,
+                                  unsigned ignore_components, int threads, j2k_plan **out) {
   if (!cs || !out || len < 2) return J2K_ERR_ARG;
   *out = nullptr;
   j2k_plan *p = new (std::nothrow) j2k_plan;
@@ -18,6 +18,7 @@ extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels
   opt.discard_levels = discard_levels < 0 ? 0 : discard_levels;
   opt.max_layers = max_layers;
   opt.ignore_components = ignore_components;
+  opt.threads = threads < 1 ? 1 : (threads > 64 ? 64 : threads);
   // the stream's sizes drive host allocations: an oversized (or corrupt but well-formed)
   // header fails here with an error code instead of an exception through the C ABI
   int rc;
@@ -36,6 +37,11 @@ extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels
   }
   *out = p;
   return J2K_OK;
+}
+
+extern "C" int j2k_plan_create(const uint8_t *cs, size_t len, int discard_levels, int max_layers,
+                               unsigned ignore_components, j2k_plan **out) {
+  return j2k_plan_create_mt(cs, len, discard_levels, max_layers, ignore_components, 1, out);
 }
 
 extern "C" void j2k_plan_destroy(j2k_plan *p) {

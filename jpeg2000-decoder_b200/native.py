@@ -104,7 +104,7 @@ _enc = None
 
 # every symbol include/j2k_gpu.h, include/bmi_jp2dec.h and include/bmi_decoder_c.h declare
 EXPORTS = [
-    "j2k_plan_create", "j2k_plan_destroy", "j2k_plan_info", "j2k_plan_cblks", "j2k_plan_seglens",
+    "j2k_plan_create", "j2k_plan_create_mt", "j2k_plan_destroy", "j2k_plan_info", "j2k_plan_cblks", "j2k_plan_seglens",
     "j2k_plan_bytes", "j2k_plan_tilecomps", "j2k_output_bytes", "j2k_status_string",
     "j2k_gpu_ctx_create", "j2k_gpu_ctx_destroy", "j2k_gpu_mem_usage", "j2k_gpu_batch_begin",
     "j2k_gpu_batch_add", "j2k_gpu_batch_footprint", "j2k_gpu_batch_launch", "j2k_gpu_batch_stage", "j2k_gpu_batch_run", "j2k_gpu_batch_sync",
@@ -130,6 +130,7 @@ def lib():
         L = ctypes.CDLL(LIB_PATH)
         vp, i, u64, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_size_t
         L.j2k_plan_create.argtypes = [ctypes.c_char_p, sz, i, i, ctypes.c_uint, ctypes.POINTER(vp)]
+        L.j2k_plan_create_mt.argtypes = [ctypes.c_char_p, sz, i, i, ctypes.c_uint, i, ctypes.POINTER(vp)]
         L.j2k_plan_destroy.argtypes = [vp]
         L.j2k_plan_destroy.restype = None
         L.j2k_plan_info.argtypes = [vp, ctypes.POINTER(ImageInfo)]
@@ -257,11 +258,11 @@ def encode(planes, bitdepth, **kw):
 class Plan:
     """Host Tier-2 result of one codestream (j2k_plan_*)."""
 
-    def __init__(self, codestream, discard_levels=0, max_layers=0, ignore_components=0):
+    def __init__(self, codestream, discard_levels=0, max_layers=0, ignore_components=0, threads=1):
         self._cs = bytes(codestream)
         self.h = ctypes.c_void_p()
-        rc = lib().j2k_plan_create(self._cs, len(self._cs), discard_levels, max_layers, ignore_components,
-                                   ctypes.byref(self.h))
+        rc = lib().j2k_plan_create_mt(self._cs, len(self._cs), discard_levels, max_layers, ignore_components,
+                                      threads, ctypes.byref(self.h))
         if rc != J2K_OK:
             raise J2kError(rc, "j2k_plan_create")
         self.info = ImageInfo()

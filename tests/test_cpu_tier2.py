@@ -223,3 +223,29 @@ def test_image_and_tile_origins(pkg):
     with pytest.raises(native.J2kError) as e:
         native.Plan(f.getvalue())
     assert e.value.code == native.J2K_ERR_UNSUPPORTED
+
+
+def test_threaded_tiles_give_identical_plans(pkg):
+    """The Tier-2 of a multi-tile picture spread over several host threads
+    (j2k_plan_create_mt) gives the same plan as one thread, at full and reduced resolution."""
+    import ctypes
+    import hashlib
+    from jpeg2000_decoder_b200 import native
+
+    def digest(cs, threads, discard):
+        p = native.Plan(cs, discard_levels=discard, threads=threads)
+        I = p.info
+        h = hashlib.sha1(bytes(I))
+        h.update(ctypes.string_at(native.lib().j2k_plan_bytes(p.h), I.coded_bytes))
+        h.update(bytes(p.cblks()))
+        h.update(ctypes.string_at(native.lib().j2k_plan_seglens(p.h), 4 * I.num_segs))
+        h.update(ctypes.string_at(native.lib().j2k_plan_tilecomps(p.h), I.num_tilecomps * ctypes.sizeof(native.TileComp)))
+        return h.hexdigest()
+
+    streams = [ts.encode_case(kw) for _, kw, _ in ts.marker_cases()] + [cs for _, cs in ts.splice_cases()]
+    streams += [ts.random_case_stream(77, i, *c)[1] for i, c in enumerate(ts.random_cases(77, 20))]
+    for cs in streams:
+        for discard in (0, 1):
+            want = digest(cs, 1, discard)
+            for threads in (2, 5):
+                assert digest(cs, threads, discard) == want
