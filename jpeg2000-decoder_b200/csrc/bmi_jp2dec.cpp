@@ -7,7 +7,10 @@
  * allocate (:420-597); BMI_dec_init fails with -1 when a pool is missing or too small
  * (dec_check_param2, :107-137); 0 / -1 return codes; BMI_dec_thumbnail returns PARSING on
  * success (:248-270, :400); BMI_dec_isr is an FPGA stub and BMI_dec_exit releases state.
- * The pools are accounted for but the device pool of the shared context does the work.
+ * The pools are accounted for but the device pool of the shared context does the work;
+ * BMI_dec_init keeps its thread count at the start of pool 0 (the reference keeps its
+ * decoder state in that pool), and BMI_dec spreads a multi-tile picture's Tier-2 over
+ * that many host threads.
  */
 #include <cstring>
 #include <mutex>
@@ -21,6 +24,20 @@ namespace {
 std::mutex g_mu;
 j2k_gpu_ctx *g_ctx = nullptr;
 
+// what BMI_dec_init leaves at the start of pool 0
+struct InitRecord {
+  uint32_t magic;
+  int32_t threads;
+};
+constexpr uint32_t kInitMagic = 0x4A324B54u;
+
+int tier2_threads(const stru_dec_param *p) {
+  if (!p->mempool[0] || p->pool_size[0] < (int)sizeof(InitRecord)) return 1;
+  InitRecord r;
+  std::memcpy(&r, p->mempool[0], sizeof(r));
+  return r.magic == kInitMagic && r.threads > 1 ? r.threads : 1;
+}
+
 j2k_gpu_ctx *ctx() {
   if (!g_ctx && j2k_gpu_ctx_create(0, 0, &g_ctx) != J2K_OK) g_ctx = nullptr;
   return g_ctx;
@@ -31,7 +48,8 @@ int decode_planes(stru_dec_param *p, void *output[MAX_COMPONENT], int discard) {
   j2k_gpu_ctx *c = ctx();
   if (!c) return -1;
   j2k_plan *plan = nullptr;
-  if (j2k_plan_create((const uint8_t *)p->input, p->in_size, discard, 0, 0, &plan) != J2K_OK) return -1;
+  if (j2k_plan_create_mt((const uint8_t *)p->input, p->in_size, discard, 0, 0, tier2_threads(p), &plan) != J2K_OK)
+    return -1;
   j2k_image_info I;
   j2k_plan_info(plan, &I);
   // colour pictures come back through the inverse MCT (RGB order), others per component
@@ -119,9 +137,11 @@ extern "C" int BMI_dec_info(stru_dec_param *p, int thread_num) {
 
 extern "C" int BMI_dec_init(stru_dec_param *p, int use_j2k_header, int thread_num) {
   (void)use_j2k_header;
-  (void)thread_num;
   if (!p) return -1;
-  if (!p->mempool[0] || !p->mempool[1] || p->pool_size[0] <= 0 || p->pool_size[1] <= 0) return -1;
+  if (!p->mempool[0] || !p->mempool[1] || p->pool_size[0] < (int)sizeof(InitRecord) || p->pool_size[1] <= 0)
+    return -1;
+  const InitRecord r{kInitMagic, thread_num > 1 ? thread_num : 1};
+  std::memcpy(p->mempool[0], &r, sizeof(r));
   std::lock_guard<std::mutex> g(g_mu);
   return ctx() ? 0 : -1;
 }

@@ -267,6 +267,23 @@ def test_bmi_dec_c_api(pkg):
     thumbs = [np.zeros((64, 64), np.uint8) for _ in range(3)]
     touts = (ctypes.c_void_p * 4)(*[pl.ctypes.data for pl in thumbs], None)
     assert L.BMI_dec_thumbnail(ctypes.byref(p), touts, 2, 1) == 1  # PARSING = success
+    # a multi-tile picture with the Tier-2 on 1 and on 4 host threads (BMI_dec_init's count)
+    cs2 = _read("rgb300x200_97_tiles_3layers.j2k")
+    buf2 = ctypes.create_string_buffer(cs2, len(cs2))
+    p.input = ctypes.cast(buf2, ctypes.c_void_p)
+    p.in_size = len(cs2)
+    assert L.BMI_dec_info(ctypes.byref(p), 4) == 0 and (p.width, p.height) == (300, 200)
+    pools = [ctypes.create_string_buffer(max(1, p.pool_size[k])) for k in range(2)]
+    p.mempool[0] = ctypes.cast(pools[0], ctypes.c_void_p)
+    p.mempool[1] = ctypes.cast(pools[1], ctypes.c_void_p)
+    got = []
+    for threads in (1, 4):
+        assert L.BMI_dec_init(ctypes.byref(p), 1, threads) == 0
+        planes = [np.zeros((200, 300), np.uint8) for _ in range(3)]
+        outs = (ctypes.c_void_p * 4)(*[pl.ctypes.data for pl in planes], None)
+        assert L.BMI_dec(ctypes.byref(p), outs, 1) == 0
+        got.append(np.stack(planes))
+    assert np.array_equal(got[0], got[1])
     assert L.BMI_dec_exit(ctypes.byref(p)) == 0
 
 
