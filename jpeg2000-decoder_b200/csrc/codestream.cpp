@@ -426,7 +426,6 @@ int finish_coding(StreamHeader &H, const StreamHeader *main) {
   for (int c = 0; c < H.ncomp; ++c) {
     if (H.cbw_exp[c] > 10 || H.cbh_exp[c] > 10 || H.cbw_exp[c] + H.cbh_exp[c] > 12) return PARSE_ERR_INVALID;
     if (H.cbw_exp[c] > 6 || H.cbh_exp[c] > 6) return PARSE_ERR_UNSUPPORTED;  // device kernels: <= 64
-    if (H.cbstyle[c] & J2K_CB_CAUSAL) return PARSE_ERR_UNSUPPORTED;
     if (H.roi_shift[c]) return PARSE_ERR_UNSUPPORTED;
     // the device runs one wavelet and one inverse MCT per image
     if (H.reversible[c] != H.reversible[0]) return PARSE_ERR_UNSUPPORTED;

@@ -501,12 +501,15 @@ struct T1Coder {
     mq.encode(cx[c], bit);
   }
 
-  void neighbours(int i, int &hh, int &vv, int &dd) const {
+  // CAUSAL (T.800 D.7): the last row of a stripe sees the next stripe as insignificant
+  bool below_cut(int y) const { return (mode & J2KENC_CAUSAL) && (y & 3) == 3; }
+  void neighbours(int i, int y, int &hh, int &vv, int &dd) const {
+    const int below = below_cut(y) ? 0 : 1;
     hh = sig[i - 1] + sig[i + 1];
-    vv = sig[i - stride] + sig[i + stride];
-    dd = sig[i - stride - 1] + sig[i - stride + 1] + sig[i + stride - 1] + sig[i + stride + 1];
+    vv = sig[i - stride] + below * sig[i + stride];
+    dd = sig[i - stride - 1] + sig[i - stride + 1] + below * (sig[i + stride - 1] + sig[i + stride + 1]);
   }
-  void code_sign(int i, bool rawmode) {
+  void code_sign(int i, int y, bool rawmode) {
     int s = sgn[i];
     if (rawmode) {
       raw.put(s);
@@ -514,7 +517,7 @@ struct T1Coder {
     }
     auto contrib = [&](int j) { return sig[j] ? (sgn[j] ? -1 : 1) : 0; };
     int H = contrib(i - 1) + contrib(i + 1);
-    int V = contrib(i - stride) + contrib(i + stride);
+    int V = contrib(i - stride) + (below_cut(y) ? 0 : contrib(i + stride));
     H = std::max(-1, std::min(1, H));
     V = std::max(-1, std::min(1, V));
     int c, xr;
@@ -529,7 +532,7 @@ struct T1Coder {
           int i = at(x, y);
           if (sig[i]) continue;
           int hh, vv, dd;
-          neighbours(i, hh, vv, dd);
+          neighbours(i, y, hh, vv, dd);
           if (hh + vv + dd == 0) continue;
           int bit = (mag[i] >> p) & 1;
           if (rawmode)
@@ -538,7 +541,7 @@ struct T1Coder {
             put(CTX_ZC + kZc.t[band][hh][vv][dd], bit);
           vis[i] = 1;
           if (bit) {
-            code_sign(i, rawmode);
+            code_sign(i, y, rawmode);
             sig[i] = 1;
             double m = mag[i], r = 1.5 * (double)(1 << p);
             dist += m * m - (m - r) * (m - r);
@@ -560,7 +563,7 @@ struct T1Coder {
               c = 2;
             } else {
               int hh, vv, dd;
-              neighbours(i, hh, vv, dd);
+              neighbours(i, y, hh, vv, dd);
               c = (hh + vv + dd) ? 1 : 0;
             }
             put(CTX_MR + c, bit);
@@ -572,13 +575,13 @@ struct T1Coder {
           dist += (m - before) * (m - before) - (m - after) * (m - after);
         }
   }
-  void code_cu_sample(int i, int p, double &dist) {
+  void code_cu_sample(int i, int y, int p, double &dist) {
     int hh, vv, dd;
-    neighbours(i, hh, vv, dd);
+    neighbours(i, y, hh, vv, dd);
     int bit = (mag[i] >> p) & 1;
     put(CTX_ZC + kZc.t[band][hh][vv][dd], bit);
     if (bit) {
-      code_sign(i, false);
+      code_sign(i, y, false);
       sig[i] = 1;
       double m = mag[i], r = 1.5 * (double)(1 << p);
       dist += m * m - (m - r) * (m - r);
@@ -596,7 +599,7 @@ struct T1Coder {
             if (sig[i] || vis[i]) run = false;
             else {
               int hh, vv, dd;
-              neighbours(i, hh, vv, dd);
+              neighbours(i, y, hh, vv, dd);
               if (hh + vv + dd) run = false;
             }
           }
@@ -615,7 +618,7 @@ struct T1Coder {
             put(CTX_UNI, (r >> 1) & 1);
             put(CTX_UNI, r & 1);
             int i = at(x, y0 + r);
-            code_sign(i, false);
+            code_sign(i, y0 + r, false);
             sig[i] = 1;
             double m = mag[i], rr = 1.5 * (double)(1 << p);
             dist += m * m - (m - rr) * (m - rr);
@@ -625,7 +628,7 @@ struct T1Coder {
         for (int y = ystart; y < ye; ++y) {
           int i = at(x, y);
           if (sig[i] || vis[i]) continue;
-          code_cu_sample(i, p, dist);
+          code_cu_sample(i, y, p, dist);
         }
       }
     if (mode & J2KENC_SEGSYM) {
@@ -907,12 +910,12 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
   if (L < 0 || L > 10) return -3;
   if (P->cbw_exp < 2 || P->cbh_exp < 2 || P->cbw_exp + P->cbh_exp > 12) return -4;
   if (P->num_layers < 1 || P->num_layers > 32) return -5;
-  if (P->mode & J2KENC_CAUSAL) return -6;
   const int TW = P->tile_w > 0 ? P->tile_w : W, TH = P->tile_h > 0 ? P->tile_h : H;
   if (P->tile_w > 0 && ((TW % (1 << L)) || (TH % (1 << L)))) return -7;  // even origins at all levels
   const bool rev = P->reversible != 0;
   const bool mct = P->use_mct && ncomp >= 3;
-  const int mode = P->mode & (J2KENC_BYPASS | J2KENC_RESET | J2KENC_TERMALL | J2KENC_PTERM | J2KENC_SEGSYM);
+  const int mode =
+      P->mode & (J2KENC_BYPASS | J2KENC_RESET | J2KENC_TERMALL | J2KENC_CAUSAL | J2KENC_PTERM | J2KENC_SEGSYM);
   int nthreads = P->num_threads > 0 ? P->num_threads : (int)std::thread::hardware_concurrency();
   if (nthreads < 1) nthreads = 1;
   const int ntx = ceil_div(W, TW), nty = ceil_div(H, TH);

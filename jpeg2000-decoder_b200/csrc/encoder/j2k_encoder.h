@@ -8,7 +8,7 @@
  * quality layers chosen by slope thresholds, LRCP/RLCP/RPCL/PCRL/CPRL progression with one
  * precinct per resolution, progression volumes (POC, main or tile-part header), tile-parts
  * (optionally interleaved across tiles), SOP / EPH markers, packed packet headers (PPM or
- * PPT), and the BYPASS / RESET / TERMALL / SEGSYM mode switches.
+ * PPT), and the BYPASS / RESET / TERMALL / CAUSAL / SEGSYM mode switches.
  *
  * The irreversible path writes one guard bit by default: the reference's Tier-1 places the
  * most significant magnitude bit at (expn - 1 - missing) (decoder/codec/src/
@@ -31,7 +31,7 @@ enum j2kenc_mode {
   J2KENC_BYPASS = 0x01,
   J2KENC_RESET = 0x02,
   J2KENC_TERMALL = 0x04,
-  J2KENC_CAUSAL = 0x08, /* not supported by this writer */
+  J2KENC_CAUSAL = 0x08, /* vertically stripe-causal contexts */
   J2KENC_PTERM = 0x10,  /* accepted, termination is the plain T.800 flush */
   J2KENC_SEGSYM = 0x20
 };

@@ -289,9 +289,13 @@ __device__ __forceinline__ int sign_index(uint32_t cw, uint32_t wl, uint32_t wr,
 }
 
 // Mark row k of the column at `wp` significant with sign `sym`: spread sigma / chi to the
-// neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).
+// neighbouring words (bmi_block_decoder.cpp:53-101 and the row 1..3 variants).  In CAUSAL
+// blocks (T.800 D.7) a stripe's last row sees the next stripe as insignificant, so row 0
+// spreads nothing upward; the flag sits in a spare byte of the refined-rows array (see
+// causal_flag) and is read only here.
+__device__ __forceinline__ uint8_t &causal_flag(const BlockSmem &b) { return b.rf[b.gap - 1]; }
 __device__ __forceinline__ void spread_sig(const BlockSmem &b, uint32_t *wp, uint32_t &cw, int k, int sym) {
-  if (k == 0) {
+  if (k == 0 && !causal_flag(b)) {
     uint32_t *up = wp - b.gap;
     up[-1] |= 0x100u << 9;
     up[0] |= (0x80u << 9) | ((uint32_t)sym << 31);
@@ -636,7 +640,11 @@ __device__ __forceinline__ int decode_block(const j2k_cblk &cb, const uint8_t *_
                               : ((h & 3) == 2 ? (ROW_CHI(2) | ROW_CHI(3)) : ROW_CHI(3));
     for (int c = lane; c < w; c += 32) *cword(b, stripes - 1, c) = m;
   }
-  if (lane == 0) init_states(b.cx, T.mq);
+  if (lane == 0) {
+    init_states(b.cx, T.mq);
+    // stripe 0's refined-rows row has three unused bytes past the last column
+    causal_flag(b) = (cb.flags & J2K_CB_CAUSAL) ? 1 : 0;
+  }
   __syncwarp();
   if (num_passes > 0 && 30 - (int)cb.missing <= 0) return 1;
 

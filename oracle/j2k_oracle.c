@@ -272,6 +272,8 @@ typedef struct {
   int32_t *sp;     /* samples, (stripes * 4) x w */
   int w, h, stripes, gap;
   int band;
+  int causal; /* CAUSAL mode switch (T.800 D.7): a stripe's last row sees the next stripe as
+                 insignificant, so a row-0 sample spreads nothing upward */
 } blk_t;
 
 static inline uint32_t *word(blk_t *b, int stripe, int col) { return b->cw + (size_t)(stripe + 1) * b->gap + 1 + col; }
@@ -307,7 +309,7 @@ static int decode_sign(blk_t *b, int s, int c, int k, mq_t *mq, ctx_t *st, raw_t
     sym = mq_decode(mq, &st[C_SIGN + ctx]) ^ flip;
   }
   /* propagate sigma / chi (bmi_block_decoder.cpp:87-96, :128-130, :158-160, :190-198) */
-  if (k == 0) {
+  if (k == 0 && !b->causal) {
     uint32_t *up = wp - b->gap;
     up[-1] |= S_BR << 9;
     up[0] |= (S_BC << 9) | ((uint32_t)sym << 31);
@@ -438,7 +440,7 @@ static int t1_block(const j2k_cblk *cb, const uint8_t *bytes, const uint32_t *se
     free(cwbuf);
     return -2;
   }
-  blk_t b = {cwbuf, sp, w, h, stripes, gap, cb->band};
+  blk_t b = {cwbuf, sp, w, h, stripes, gap, cb->band, (cb->flags & J2K_CB_CAUSAL) != 0};
   /* OOB words after every stripe row and a partial last stripe (bmi_block_decoder.cpp:616-705) */
   const uint32_t oob = ROW_CHI(0) | ROW_CHI(1) | ROW_CHI(2) | ROW_CHI(3);
   for (int s = 0; s < stripes; ++s) {

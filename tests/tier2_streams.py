@@ -129,7 +129,8 @@ def as_rgb(out, h=H, w=W):
 
 def random_cases(seed, n):
     """(keywords, bit depth, height, width) of `n` seeded lossless encoder configurations:
-    levels 0-4, code-block sizes 4..64, 1-5 layers, mode switches, all progressions, tiles
+    levels 0-4, code-block sizes 4..64, 1-5 layers, mode switches (CAUSAL included), all
+    progressions, tiles
     of any multiple of 2^levels (the coarsest LL band may start on an odd coordinate),
     SOP / EPH, PPM or PPT, tile-parts (interleaved or not) and POC volumes covering every
     packet."""
@@ -144,7 +145,8 @@ def random_cases(seed, n):
         NL = rng.randint(1, 5)
         bpp = sorted(rng.uniform(0.3, 6) for _ in range(NL - 1)) + [0]
         kw = dict(reversible=1, levels=L, num_layers=NL, layer_bpp=bpp, cbw_exp=rng.randint(2, 6),
-                  cbh_exp=rng.randint(2, 6), mode=rng.choice([0, 1, 2, 3, 4, 0x20, 0x33, 0x37]),
+                  cbh_exp=rng.randint(2, 6),
+                  mode=rng.choice([0, 1, 2, 3, 4, 0x08, 0x0B, 0x20, 0x2C, 0x33, 0x37, 0x2F]),
                   progression=rng.randrange(5))
         kw["cbh_exp"] = min(kw["cbh_exp"], 12 - kw["cbw_exp"])
         if rng.random() < 0.6:
