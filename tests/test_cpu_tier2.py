@@ -249,3 +249,18 @@ def test_threaded_tiles_give_identical_plans(pkg):
             want = digest(cs, 1, discard)
             for threads in (2, 5):
                 assert digest(cs, threads, discard) == want
+
+
+@pytest.mark.parametrize("mode", [0x08, 0x09, 0x0E, 0x28, 0x2F])
+def test_causal_mode_streams(pkg, mode):
+    """CAUSAL (T.800 D.7), alone and with the other mode switches: OpenJPEG decodes the
+    encoder's stream to its source (the contexts are the standard's), and so does the
+    oracle from the library's plan."""
+    from jpeg2000_decoder_b200 import native
+    img = ts.source()
+    cs = native.encode(img, 8, reversible=1, levels=3, cbw_exp=4, cbh_exp=5, mode=mode, num_layers=2,
+                       layer_bpp=[1.0, 0])
+    assert np.array_equal(_oracle_rgb(cs, ts.H, ts.W).transpose(2, 0, 1), img)
+    Image = pytest.importorskip("PIL.Image")
+    ref = np.asarray(Image.open(io.BytesIO(cs)).convert("RGB"))
+    assert np.array_equal(ref.transpose(2, 0, 1), img)
