@@ -1054,6 +1054,9 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
 
     // ---- emit plan entries for this tile (offsets relative to the tile)
     size_t tile_bytes = 0;
+    out.spans.reserve(pieces.size());
+    out.cblks.reserve(tile_blocks);
+    out.seglens.reserve(segs.size());
     for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       if ((opt.ignore_components >> c) & 1) continue;
