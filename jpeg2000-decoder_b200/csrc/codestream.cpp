@@ -174,7 +174,6 @@ struct BandState {
   int off_x, off_y;         // position inside the tile-component Mallat region
   // code-blocks grouped by precinct
   std::vector<std::vector<int>> prec_cbs;   // [precinct] -> indices into cbs
-  std::vector<int> prec_gw, prec_gh;        // code-block grid of each precinct
   std::vector<TagTree> incl, zbp;
   std::vector<CbState> cbs;
 };
@@ -785,8 +784,6 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
           // precincts and code-blocks
           int np = R.npx * R.npy;
           B.prec_cbs.assign(np, {});
-          B.prec_gw.assign(np, 0);
-          B.prec_gh.assign(np, 0);
           B.incl.assign(np, TagTree());
           B.zbp.assign(np, TagTree());
           if (B.x1 <= B.x0 || B.y1 <= B.y0) continue;
@@ -802,8 +799,6 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
               if (bx1 <= bx0 || by1 <= by0) continue;
               int cx0 = bx0 >> cbw, cx1 = (bx1 + (1 << cbw) - 1) >> cbw;
               int cy0 = by0 >> cbh, cy1 = (by1 + (1 << cbh) - 1) >> cbh;
-              B.prec_gw[p] = cx1 - cx0;
-              B.prec_gh[p] = cy1 - cy0;
               B.incl[p].build(cx1 - cx0, cy1 - cy0);
               B.zbp[p].build(cx1 - cx0, cy1 - cy0);
               for (int cy = cy0; cy < cy1; ++cy)
@@ -871,20 +866,24 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       BitReader br = pk ? BitReader{hcur, hend} : BitReader{cur, end};
       contribs.clear();
       lens.clear();
+      const int style = TH.cbstyle[c];
+      const bool one_segment = !(style & (J2K_CB_BYPASS | J2K_CB_TERMALL));
       if (br.bit()) {
         for (auto &B : R.bands) {
           if (B.prec_cbs.empty() || B.prec_cbs[p].empty()) continue;
-          int gw = B.prec_gw[p];
-          for (size_t k = 0; k < B.prec_cbs[p].size(); ++k) {
-            CbState &cb = B.cbs[B.prec_cbs[p][k]];
+          const std::vector<int> &members = B.prec_cbs[p];
+          TagTree &incl_tree = B.incl[p];
+          TagTree &zbp_tree = B.zbp[p];
+          for (size_t k = 0; k < members.size(); ++k) {
+            CbState &cb = B.cbs[members[k]];
             int incl;
-            if (!cb.included) incl = B.incl[p].decode(br, (int)k, l + 1);
+            if (!cb.included) incl = incl_tree.decode(br, (int)k, l + 1);
             else incl = br.bit();
             if (br.overrun) return PARSE_ERR_PACKET;
             if (!incl) continue;
             if (!cb.included) {
               int i = 0;
-              while (!B.zbp[p].decode(br, (int)k, i)) {
+              while (!zbp_tree.decode(br, (int)k, i)) {
                 ++i;
                 if (br.overrun || i > 74) return PARSE_ERR_PACKET;
               }
@@ -907,20 +906,26 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
               if (++cb.lblock > 32 || br.overrun) return PARSE_ERR_PACKET;
             }
             Contrib ct{&cb, (uint32_t)lens.size(), 0, n, 0};
-            int s = cb.passes;
-            while (s < cb.passes + n) {
-              int e = s + 1;
-              while (e < cb.passes + n && !seg_starts(TH.cbstyle[c], e)) ++e;
-              int nb = cb.lblock + floor_log2((uint32_t)(e - s));
+            if (one_segment) {  // every pass in the block's single codeword segment
+              const int nb = cb.lblock + floor_log2((uint32_t)n);
               if (nb > 32) return PARSE_ERR_PACKET;
               lens.push_back(br.bits(nb));
-              if (s == cb.passes) ct.first_seg_new = seg_starts(TH.cbstyle[c], s);
-              s = e;
+              ct.first_seg_new = cb.passes == 0;
+            } else {
+              int s = cb.passes;
+              while (s < cb.passes + n) {
+                int e = s + 1;
+                while (e < cb.passes + n && !seg_starts(style, e)) ++e;
+                const int nb = cb.lblock + floor_log2((uint32_t)(e - s));
+                if (nb > 32) return PARSE_ERR_PACKET;
+                lens.push_back(br.bits(nb));
+                if (s == cb.passes) ct.first_seg_new = seg_starts(style, s);
+                s = e;
+              }
             }
             if (br.overrun) return PARSE_ERR_PACKET;
             ct.nlens = (uint32_t)lens.size() - ct.lens_at;
             contribs.push_back(ct);
-            (void)gw;
           }
         }
       }
