@@ -346,6 +346,19 @@ def run_gpu(args, rank, world, dist):
         roof_t1["decisions_per_px"] = round(dpp, 3)
     roof_t1["compressed_bytes_per_s"] = round(coded / (t1_ms / 1e3), 1)
     clocks = clk.summary()
+    # Tier-1 is bound by instruction issue: its own roofline is warp instructions issued per
+    # second (live decisions/s x the warp instructions per decision of the profiled compact
+    # form) against 4 issue slots per SM per cycle at the sampled SM clock
+    roof_t1_issue = None
+    ipd = tr.get("t1_warp_inst_per_decision")
+    if dpp and ipd and tuned and tuned["t1_form"] == 1 and clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        peak_issue = sms * 4 * clocks["sm_mhz"] * 1e6
+        achieved = dpp * pixels / (t1_ms / 1e3) * ipd
+        roof_t1_issue = {"bound": "issue", "achieved": round(achieved / 1e9, 1), "peak": round(peak_issue / 1e9, 1),
+                         "unit": "Gwarp-inst/s", "frac": round(achieved / peak_issue, 4),
+                         "warp_inst_per_decision": ipd, "kernel": "t1_kernel_compact",
+                         "source": "profiles/traffic.json (ncu instruction count of the same kernel)"}
     cfg = dict(cfg)
     cfg.update({"parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",
                 "bad_blocks": bad, "cuda_graph": not args.no_graph,
@@ -365,7 +378,7 @@ def run_gpu(args, rank, world, dist):
                                "what": "one image per launch sequence, host buffers"},
             "speedup_vs_plain": round(value / plain, 2),
             "roofline": roof_t1 if dominant == "t1" else roof_dwt,
-            "roofline_dwt": roof_dwt, "roofline_t1": roof_t1,
+            "roofline_dwt": roof_dwt, "roofline_t1": roof_t1, "roofline_t1_issue": roof_t1_issue,
             "stage_ms": {"t1": round(t1_ms, 4), "dwt_mct": round(dwt_ms, 4)},
             "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
                              "sample": sample},
