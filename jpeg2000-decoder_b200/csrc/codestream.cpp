@@ -229,6 +229,17 @@ void copy_chunks(const std::vector<CopyChunk> &chunks, size_t total) {
   for (auto &x : th) x.join();
 }
 
+// First pass after pass s that starts a new codeword segment (T.800 D.4.1 and D.6): every
+// pass with TERMALL; with BYPASS, passes 0-9 share the first (MQ) segment and later ones
+// alternate a raw segment (significance + refinement) and an MQ one (cleanup); otherwise no
+// later segment
+int next_seg_start(int style, int s) {
+  if (style & J2K_CB_TERMALL) return s + 1;
+  if (!(style & J2K_CB_BYPASS)) return 1 << 30;
+  if (s < 10) return 10;
+  return ((s - 1) % 3 == 0) ? s + 2 : s + 1;
+}
+
 bool seg_starts(int style, int j) {
   int type = (j == 0) ? 2 : (j - 1) % 3;
   if (j == 0) return true;
@@ -914,8 +925,7 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             } else {
               int s = cb.passes;
               while (s < cb.passes + n) {
-                int e = s + 1;
-                while (e < cb.passes + n && !seg_starts(style, e)) ++e;
+                const int e = std::min(next_seg_start(style, s), cb.passes + n);
                 const int nb = cb.lblock + floor_log2((uint32_t)(e - s));
                 if (nb > 32) return PARSE_ERR_PACKET;
                 lens.push_back(br.bits(nb));
