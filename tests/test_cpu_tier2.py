@@ -264,3 +264,31 @@ def test_causal_mode_streams(pkg, mode):
     Image = pytest.importorskip("PIL.Image")
     ref = np.asarray(Image.open(io.BytesIO(cs)).convert("RGB"))
     assert np.array_equal(ref.transpose(2, 0, 1), img)
+
+
+def test_plain_c_caller_of_the_c_abi(pkg):
+    """A C99 program including every public header, linked against the library, plans a
+    codestream through the C ABI (one and three threads give the same plan), sees the
+    error codes, and gets J2K_ERR_NODEVICE (or a context, on a GPU host) for a device
+    context."""
+    import shutil
+    import subprocess
+    from jpeg2000_decoder_b200 import native
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("no C compiler")
+    out_dir = os.path.join(ROOT, "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, "c_abi_consumer")
+    lib_dir = os.path.dirname(native.LIB_PATH)
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_abi_consumer.c"), "-L", lib_dir, "-l:" + os.path.basename(native.LIB_PATH),
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    name = os.path.join(ROOT, "tests", "golden", "rgb300x200_97_tiles_3layers.j2k")
+    r = subprocess.run([exe, name], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    w, h, ncomp, cblks, coded, ctx_rc = (int(x) for x in r.stdout.split())
+    plan = native.Plan(open(name, "rb").read())
+    assert (w, h, ncomp, cblks, coded) == (plan.info.width, plan.info.height, plan.info.ncomp,
+                                           plan.info.num_cblks, plan.info.coded_bytes)
+    assert ctx_rc in (native.J2K_OK, native.J2K_ERR_NODEVICE)
