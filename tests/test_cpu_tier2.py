@@ -292,3 +292,38 @@ def test_plain_c_caller_of_the_c_abi(pkg):
     assert (w, h, ncomp, cblks, coded) == (plan.info.width, plan.info.height, plan.info.ncomp,
                                            plan.info.num_cblks, plan.info.coded_bytes)
     assert ctx_rc in (native.J2K_OK, native.J2K_ERR_NODEVICE)
+
+
+def test_plan_builder_under_sanitizers(pkg):
+    """The plan builder built with AddressSanitizer + UndefinedBehaviorSanitizer plans or
+    refuses 1500 seeded corruptions of the Tier-2 variant streams without a report."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no C++ compiler")
+    out_dir = os.path.join(ROOT, "_build", "asan")
+    seed_dir = os.path.join(out_dir, "seeds")
+    os.makedirs(seed_dir, exist_ok=True)
+    streams = []
+    for name in sorted(os.listdir(FIX)):
+        if name.endswith(".j2k"):
+            with open(os.path.join(FIX, name), "rb") as f:
+                streams.append(f.read())
+    streams += [ts.encode_case(kw) for _, kw, _ in ts.marker_cases()]
+    streams += [ts.random_case_stream(99, i, *c)[1] for i, c in enumerate(ts.random_cases(99, 12))]
+    for i, cs in enumerate(streams):
+        with open(os.path.join(seed_dir, "s%03d.j2k" % i), "wb") as f:
+            f.write(cs)
+    csrc = os.path.join(ROOT, "jpeg2000-decoder_b200", "csrc")
+    exe = os.path.join(out_dir, "asan_plan_fuzz")
+    build = subprocess.run([gxx, "-O1", "-g", "-std=c++17", "-pthread", "-fsanitize=address,undefined",
+                            "-fno-omit-frame-pointer", "-I", os.path.join(ROOT, "include"), "-I", csrc,
+                            os.path.join(ROOT, "tests", "asan_plan_fuzz.cpp"), os.path.join(csrc, "codestream.cpp"),
+                            os.path.join(csrc, "plan_api.cpp"), "-o", exe], capture_output=True, text=True)
+    if build.returncode != 0 and "sanitize" in build.stderr:
+        pytest.skip("no sanitizer runtime")
+    assert build.returncode == 0, build.stderr[-2000:]
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
+    r = subprocess.run([exe, seed_dir, "7", "1500"], capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0 and "planned" in r.stdout, (r.stdout + r.stderr)[-3000:]
