@@ -542,6 +542,9 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   for (int c = 0; c < H.ncomp; ++c) {
     if (H.sub_x[c] != 1 || H.sub_y[c] != 1) return PARSE_ERR_UNSUPPORTED;
     if (H.depth[c] > 16 || H.depth[c] != H.depth[0]) return PARSE_ERR_UNSUPPORTED;
+    // signed samples take no DC level shift (T.800 G.1.2); the output stages apply the
+    // unsigned shift, so such pictures are refused rather than decoded wrongly
+    if (H.is_signed[c]) return PARSE_ERR_UNSUPPORTED;
   }
   int rc = finish_coding(H, nullptr);
   if (rc != PARSE_OK) return rc;

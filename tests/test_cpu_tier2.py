@@ -79,7 +79,8 @@ def test_tile_header_coding_overrides(pkg, case):
 
 
 def test_refusals(pkg):
-    """A tile that switches the wavelet, POC with a broken length, PPM and PPT together."""
+    """A tile that switches the wavelet, POC with a broken length, signed samples, PPM and PPT
+    together."""
     from jpeg2000_decoder_b200 import native
     with pytest.raises(native.J2kError) as e:
         native.Plan(ts.transform_mismatch_stream())
@@ -89,6 +90,12 @@ def test_refusals(pkg):
     cs[i + 3] += 1  # Lpoc no longer a whole number of entries
     with pytest.raises(native.J2kError):
         native.Plan(bytes(cs))
+    signed = bytearray(ts.encode_case(dict()))
+    i = signed.find(b"\xff\x51") + 40  # Ssiz of component 0
+    signed[i] |= 0x80
+    with pytest.raises(native.J2kError) as e:
+        native.Plan(bytes(signed))
+    assert e.value.code == native.J2K_ERR_UNSUPPORTED
     ppm = ts.encode_case(dict(markers=native.ENC_PPM))
     ppt = ts.encode_case(dict(markers=native.ENC_PPT))
     segs, sot = ts._segments(ppm, 2)
