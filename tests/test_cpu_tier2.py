@@ -334,3 +334,17 @@ def test_plan_builder_under_sanitizers(pkg):
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
     r = subprocess.run([exe, seed_dir, "7", "1500"], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0 and "planned" in r.stdout, (r.stdout + r.stderr)[-3000:]
+
+
+@pytest.mark.parametrize("depth", [1, 2, 15, 16])
+def test_bit_depth_extremes_lossless(pkg, depth):
+    """1, 2, 15 and 16-bit lossless pictures (with and without BYPASS+RESET) decode to
+    their sources through the plan and the oracle."""
+    from jpeg2000_decoder_b200 import native, synth
+    img = synth.fractal_rgb(3, 70, 90, bitdepth=depth)
+    for mode in (0, 3):
+        cs = native.encode(img, depth, reversible=1, levels=3, mode=mode)
+        rc, out, _ = oracle_util.oracle_decode(native.Plan(cs), native.FMT_48BITS_RGB)
+        assert rc == 0
+        rgb = out.view(np.uint16).reshape(70, 90, 3)[:, :, ::-1].transpose(2, 0, 1) >> (16 - depth)
+        assert np.array_equal(rgb, img), (depth, mode)

@@ -427,3 +427,16 @@ def test_randomized_encoder_configurations_bit_exact(gpu_ctx):
         fmt = native.FMT_24BITS_RGB if depth == 8 else native.FMT_48BITS_RGB
         out, plan = _decode_check(gpu_ctx, cs, fmt)
         assert np.array_equal(ts.rgb_of(out, depth, h, w), img), (i, kw)
+
+
+@pytest.mark.parametrize("depth", [1, 16])
+def test_bit_depth_extremes_bit_exact(gpu_ctx, depth):
+    """1-bit and 16-bit lossless pictures decode on the device as the oracle decodes them
+    and reproduce their sources."""
+    from jpeg2000_decoder_b200 import native, synth
+    img = synth.fractal_rgb(3, 70, 90, bitdepth=depth)
+    for mode in (0, 3):
+        cs = native.encode(img, depth, reversible=1, levels=3, mode=mode)
+        out, _ = _decode_check(gpu_ctx, cs, native.FMT_48BITS_RGB)
+        rgb = out.view(np.uint16).reshape(70, 90, 3)[:, :, ::-1].transpose(2, 0, 1) >> (16 - depth)
+        assert np.array_equal(rgb, img), (depth, mode)
