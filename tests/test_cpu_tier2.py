@@ -324,13 +324,17 @@ def test_plan_builder_under_sanitizers(pkg):
             f.write(cs)
     csrc = os.path.join(ROOT, "jpeg2000-decoder_b200", "csrc")
     exe = os.path.join(out_dir, "asan_plan_fuzz")
-    build = subprocess.run([gxx, "-O1", "-g", "-std=c++17", "-pthread", "-fsanitize=address,undefined",
-                            "-fno-omit-frame-pointer", "-I", os.path.join(ROOT, "include"), "-I", csrc,
-                            os.path.join(ROOT, "tests", "asan_plan_fuzz.cpp"), os.path.join(csrc, "codestream.cpp"),
-                            os.path.join(csrc, "plan_api.cpp"), "-o", exe], capture_output=True, text=True)
-    if build.returncode != 0 and "sanitize" in build.stderr:
-        pytest.skip("no sanitizer runtime")
-    assert build.returncode == 0, build.stderr[-2000:]
+    srcs = [os.path.join(ROOT, "tests", "asan_plan_fuzz.cpp"), os.path.join(csrc, "codestream.cpp"),
+            os.path.join(csrc, "plan_api.cpp")]
+    deps = srcs + [os.path.join(csrc, "codestream.h"), os.path.join(csrc, "plan.h"),
+                   os.path.join(ROOT, "include", "j2k_gpu.h")]
+    if not os.path.exists(exe) or os.path.getmtime(exe) < max(os.path.getmtime(d) for d in deps):
+        build = subprocess.run([gxx, "-O1", "-g", "-std=c++17", "-pthread", "-fsanitize=address,undefined",
+                                "-fno-omit-frame-pointer", "-I", os.path.join(ROOT, "include"), "-I", csrc] + srcs +
+                               ["-o", exe], capture_output=True, text=True)
+        if build.returncode != 0 and "sanitize" in build.stderr:
+            pytest.skip("no sanitizer runtime")
+        assert build.returncode == 0, build.stderr[-2000:]
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=1", UBSAN_OPTIONS="print_stacktrace=1:halt_on_error=1")
     r = subprocess.run([exe, seed_dir, "7", "1500"], capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0 and "planned" in r.stdout, (r.stdout + r.stderr)[-3000:]
