@@ -100,20 +100,22 @@ struct TagTree {
   void build(int w, int h) {
     nodes.clear();
     if (w <= 0 || h <= 0) return;
-    std::vector<std::pair<int, int>> dims{{w, h}};
-    while (dims.back().first > 1 || dims.back().second > 1)
-      dims.push_back({(dims.back().first + 1) / 2, (dims.back().second + 1) / 2});
-    std::vector<int> base;
-    int total = 0;
-    for (auto &d : dims) {
-      base.push_back(total);
-      total += d.first * d.second;
+    // level sizes halve up to a single root: at most 32 levels for 31-bit sizes
+    int dw[34], dh[34], base[34], nl = 0, total = 0;
+    dw[0] = w;
+    dh[0] = h;
+    for (;;) {
+      base[nl] = total;
+      total += dw[nl] * dh[nl];
+      if (dw[nl] == 1 && dh[nl] == 1) break;
+      dw[nl + 1] = (dw[nl] + 1) / 2;
+      dh[nl + 1] = (dh[nl] + 1) / 2;
+      ++nl;
     }
     nodes.assign(total, {1 << 30, 0, -1});
-    for (size_t l = 0; l + 1 < dims.size(); ++l)
-      for (int y = 0; y < dims[l].second; ++y)
-        for (int x = 0; x < dims[l].first; ++x)
-          nodes[base[l] + y * dims[l].first + x].parent = base[l + 1] + (y / 2) * dims[l + 1].first + x / 2;
+    for (int l = 0; l < nl; ++l)
+      for (int y = 0; y < dh[l]; ++y)
+        for (int x = 0; x < dw[l]; ++x) nodes[base[l] + y * dw[l] + x].parent = base[l + 1] + (y / 2) * dw[l + 1] + x / 2;
   }
   // returns 1 when the leaf value is below `threshold` (T.800 B.10.2)
   int decode(BitReader &br, int leaf, int threshold) {
@@ -801,6 +803,9 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
           B.incl.assign(np, TagTree());
           B.zbp.assign(np, TagTree());
           if (B.x1 <= B.x0 || B.y1 <= B.y0) continue;
+          // every code-block lies in one precinct (precinct edges are on the block grid)
+          B.cbs.reserve((size_t)(((B.x1 + (1 << cbw) - 1) >> cbw) - (B.x0 >> cbw)) *
+                        (size_t)(((B.y1 + (1 << cbh) - 1) >> cbh) - (B.y0 >> cbh)));
           // precinct size in band coordinates
           int pbx = r == 0 ? ppx : ppx - 1, pby = r == 0 ? ppy : ppy - 1;
           int px0 = R.x0 >> ppx, py0 = R.y0 >> ppy;
@@ -815,6 +820,7 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
               int cy0 = by0 >> cbh, cy1 = (by1 + (1 << cbh) - 1) >> cbh;
               B.incl[p].build(cx1 - cx0, cy1 - cy0);
               B.zbp[p].build(cx1 - cx0, cy1 - cy0);
+              B.prec_cbs[p].reserve((size_t)(cx1 - cx0) * (cy1 - cy0));
               for (int cy = cy0; cy < cy1; ++cy)
                 for (int cx = cx0; cx < cx1; ++cx) {
                   CbState cb;
