@@ -1193,17 +1193,23 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
   std::vector<CopyChunk> chunks;
   for (TileOut &o : outs) {
     const uint32_t seg_base = (uint32_t)P.seglens.size();
-    for (j2k_tilecomp tc : o.tcs) {
-      tc.coef_off += coef_total;
-      P.tilecomps.push_back(tc);
+    if (ntiles == 1) {  // one tile: every offset is already the plan's
+      P.tilecomps = std::move(o.tcs);
+      P.cblks = std::move(o.cblks);
+      P.seglens = std::move(o.seglens);
+    } else {
+      for (j2k_tilecomp tc : o.tcs) {
+        tc.coef_off += coef_total;
+        P.tilecomps.push_back(tc);
+      }
+      for (j2k_cblk d : o.cblks) {
+        d.out_off += coef_total;
+        d.data_off += (uint32_t)byte_base;
+        d.seg_off += seg_base;
+        P.cblks.push_back(d);
+      }
+      P.seglens.insert(P.seglens.end(), o.seglens.begin(), o.seglens.end());
     }
-    for (j2k_cblk d : o.cblks) {
-      d.out_off += coef_total;
-      d.data_off += (uint32_t)byte_base;
-      d.seg_off += seg_base;
-      P.cblks.push_back(d);
-    }
-    P.seglens.insert(P.seglens.end(), o.seglens.begin(), o.seglens.end());
     // chunks of about 1 MB of this tile's spans
     uint8_t *dst = P.bytes.data() + byte_base;
     const auto *b = o.spans.data(), *e = o.spans.data() + o.spans.size();
