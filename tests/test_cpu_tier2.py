@@ -352,3 +352,34 @@ def test_bit_depth_extremes_lossless(pkg, depth):
         assert rc == 0
         rgb = out.view(np.uint16).reshape(70, 90, 3)[:, :, ::-1].transpose(2, 0, 1) >> (16 - depth)
         assert np.array_equal(rgb, img), (depth, mode)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(tile_size=(64, 48), num_resolutions=4),
+                                dict(precinct_size=(32, 32), codeblock_size=(16, 16), progression="PCRL",
+                                     num_resolutions=4),
+                                dict(precinct_size=(16, 16), codeblock_size=(8, 8), progression="RPCL",
+                                     tile_size=(64, 64), num_resolutions=3)],
+                         ids=["one_tile", "tiles", "precincts_pcrl", "precincts_rpcl_tiles"])
+def test_openjpeg_16bit_gray_identical(pkg, kw):
+    """16-bit grayscale 5/3 streams written by OpenJPEG: the plan + oracle reconstruct the
+    same integers as OpenJPEG's own decoder (checked against its decode rather than the
+    source, which OpenJPEG's writer does not reproduce exactly for every tiling)."""
+    Image = pytest.importorskip("PIL.Image")
+    import warnings
+    from jpeg2000_decoder_b200 import native, synth
+    g = synth.fractal_rgb(5, 90, 120, bitdepth=16)[0].astype(np.uint16)
+    f = io.BytesIO()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", DeprecationWarning)
+        Image.fromarray(g, "I;16").save(f, "JPEG2000", no_jp2=True, **kw)
+    cs = f.getvalue()
+    ref = np.asarray(Image.open(io.BytesIO(cs))).astype(np.int64)
+    plan = native.Plan(cs)
+    I = plan.info
+    assert (I.bitdepth, I.ncomp, I.reversible) == (16, 1, 1)
+    rc, _, comp = oracle_util.oracle_decode(plan, native.FMT_NONE)
+    assert rc == 0
+    img = np.zeros((I.height, I.width), np.int64)
+    for tc in plan.tilecomps():
+        img[tc.y0:tc.y0 + tc.h, tc.x0:tc.x0 + tc.w] = comp[tc.coef_off:tc.coef_off + tc.w * tc.h].reshape(tc.h, tc.w)
+    assert np.array_equal(img + (1 << 15), ref)
