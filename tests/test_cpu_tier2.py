@@ -383,3 +383,32 @@ def test_openjpeg_16bit_gray_identical(pkg, kw):
     for tc in plan.tilecomps():
         img[tc.y0:tc.y0 + tc.h, tc.x0:tc.x0 + tc.w] = comp[tc.coef_off:tc.coef_off + tc.w * tc.h].reshape(tc.h, tc.w)
     assert np.array_equal(img + (1 << 15), ref)
+
+
+@pytest.mark.parametrize("kw", [dict(quality_layers=[8], quality_mode="rates"),
+                                dict(quality_layers=[3], quality_mode="rates", tile_size=(64, 64), num_resolutions=4),
+                                dict()], ids=["rate8", "rate3_tiles", "near_lossless"])
+def test_openjpeg_16bit_gray_97_within_two(pkg, kw):
+    """16-bit grayscale 9/7 streams written by OpenJPEG (two guard bits): the oracle's float
+    reconstruction, rounded, is within 2 of OpenJPEG's decode out of 65535 (the two 9/7
+    implementations order their float operations differently)."""
+    Image = pytest.importorskip("PIL.Image")
+    import warnings
+    from jpeg2000_decoder_b200 import native, synth
+    g = synth.fractal_rgb(5, 90, 120, bitdepth=16)[0].astype(np.uint16)
+    f = io.BytesIO()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", DeprecationWarning)
+        Image.fromarray(g, "I;16").save(f, "JPEG2000", no_jp2=True, irreversible=True, **kw)
+    cs = f.getvalue()
+    ref = np.asarray(Image.open(io.BytesIO(cs))).astype(np.int64)
+    plan = native.Plan(cs)
+    I = plan.info
+    rc, _, comp = oracle_util.oracle_decode(plan, native.FMT_NONE)
+    assert rc == 0 and I.reversible == 0
+    img = np.zeros((I.height, I.width), np.float64)
+    for tc in plan.tilecomps():
+        img[tc.y0:tc.y0 + tc.h, tc.x0:tc.x0 + tc.w] = \
+            comp.view(np.float32)[tc.coef_off:tc.coef_off + tc.w * tc.h].reshape(tc.h, tc.w)
+    ours = np.clip(np.floor(img + 0.5) + (1 << 15), 0, 65535).astype(np.int64)
+    assert np.abs(ours - ref).max() <= 2
