@@ -412,3 +412,23 @@ def test_openjpeg_16bit_gray_97_within_two(pkg, kw):
             comp.view(np.float32)[tc.coef_off:tc.coef_off + tc.w * tc.h].reshape(tc.h, tc.w)
     ours = np.clip(np.floor(img + 0.5) + (1 << 15), 0, 65535).astype(np.int64)
     assert np.abs(ours - ref).max() <= 2
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(tile_size=(64, 48), precinct_size=(32, 32), codeblock_size=(16, 16),
+                                             progression="CPRL", num_resolutions=4)], ids=["one_tile", "tiles_cprl"])
+def test_openjpeg_rgba_four_components(pkg, kw):
+    """4-component (RGBA) streams written by OpenJPEG decode exactly into both 32-bit packed
+    formats, component c in byte 3 - c (the layout of the reference's 4-component merge)."""
+    Image = pytest.importorskip("PIL.Image")
+    from jpeg2000_decoder_b200 import native, synth
+    rgb = np.moveaxis(synth.fields_and_edges(8, 70, 90).astype(np.uint8), 0, -1)
+    a = synth.fractal_rgb(9, 70, 90, bitdepth=8)[0].astype(np.uint8)
+    rgba = np.ascontiguousarray(np.dstack([rgb, a]))
+    f = io.BytesIO()
+    Image.fromarray(rgba, "RGBA").save(f, "JPEG2000", no_jp2=True, **kw)
+    plan = native.Plan(f.getvalue())
+    assert plan.info.ncomp == 4
+    for fmt in (native.FMT_32BITS_ARGB, native.FMT_32BITS_4COMPONENTS):
+        rc, out, _ = oracle_util.oracle_decode(plan, fmt)
+        assert rc == 0
+        assert np.array_equal(out.reshape(70, 90, 4)[:, :, ::-1], rgba)
