@@ -37,7 +37,7 @@ int main(int argc, char **argv) {
       int k = rng() % 5;
       if (k == 0) cs[rng() % std::min<size_t>(cs.size(), 600)] = rng() & 255;
       else if (k == 1) { int c = 1 + rng() % 16; for (int i = 0; i < c; ++i) cs[rng() % cs.size()] = rng() & 255; }
-      else if (k == 2) cs.resize(2 + rng() % (cs.size() - 2));
+      else if (k == 2) { if (cs.size() > 2) cs.resize(2 + rng() % (cs.size() - 2)); }
       else if (k == 3) { size_t j = rng() % cs.size(); int c = 1 + rng() % 8; for (int i = 0; i < c; ++i) cs.insert(cs.begin() + j, rng() & 255); }
       else { size_t j = rng() % cs.size(); size_t c = std::min<size_t>(1 + rng() % 8, cs.size() - j); if (cs.size() - c >= 2) cs.erase(cs.begin() + j, cs.begin() + j + c); }
     }
