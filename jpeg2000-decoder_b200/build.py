@@ -2,7 +2,9 @@
 
 libj2k_b200.so  host front end (Tier-2), BMI decoder API and the sm_100a kernels
 libj2kenc.so    the test/benchmark codestream writer
-oracle/liboracle.so and oracle/_ref/libref_t1.so are built by `build_oracle` (test infrastructure).
+oracle/liboracle.so, and with a reference tree oracle/_ref/libref_t1.so (its Tier-1) and
+oracle/_ref/libref_cpu.so (its whole CPU decoder), are built by `build_oracle`: test and
+baseline infrastructure, never linked by the product.
 """
 import os
 import shutil
@@ -19,6 +21,7 @@ LIB = os.path.join(PKG, "libj2k_b200.so")
 ENC = os.path.join(PKG, "libj2kenc.so")
 ORACLE = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_T1 = os.path.join(ROOT, "oracle", "_ref", "libref_t1.so")
+REF_CPU = os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")
 
 CU_SOURCES = ["engine.cu", "noalloc.cu"]
 CPP_SOURCES = ["codestream.cpp", "plan_api.cpp", "bmi_decoder.cpp", "bmi_jp2dec.cpp", "server.cpp"]
@@ -78,15 +81,22 @@ def build_library(force=False, verbose=False):
     return LIB
 
 
-def build_oracle(force=False, reference="/root/reference"):
-    """CPU restatement (always) and the reference's own Tier-1 (when the tree is present)."""
+def build_oracle(force=False, reference=None):
+    """CPU restatement (always); the reference's Tier-1 and whole CPU decoder when a
+    reference tree is given (argument, or the J2K_REFERENCE_DIR environment variable)."""
     src = os.path.join(ROOT, "oracle", "j2k_oracle.c")
     if force or _stale(ORACLE, [src, os.path.join(ROOT, "oracle", "j2k_oracle.h")]):
         _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-o", ORACLE, src])
-    if os.path.isdir(os.path.join(reference, "decoder")):
-        drv = os.path.join(ROOT, "oracle", "ref_t1_driver.cpp")
-        if force or _stale(REF_T1, [drv]):
-            _run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh"), reference])
+    reference = reference or os.environ.get("J2K_REFERENCE_DIR")
+    if reference and os.path.isdir(os.path.join(reference, "decoder")):
+        odir = os.path.join(ROOT, "oracle")
+        drv = os.path.join(odir, "ref_t1_driver.cpp")
+        if force or _stale(REF_T1, [drv, os.path.join(odir, "build_ref.sh")]):
+            _run(["sh", os.path.join(odir, "build_ref.sh"), reference])
+        deps = [os.path.join(odir, f) for f in ("build_ref_cpu.sh", "ref_cpu_driver.cpp", "ref_cpu_dwt_unit.cpp",
+                                                "ref_gpu_stub.c")]
+        if force or _stale(REF_CPU, deps):
+            _run(["sh", os.path.join(odir, "build_ref_cpu.sh"), reference])
     return ORACLE
 
 

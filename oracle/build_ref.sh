@@ -1,9 +1,10 @@
 #!/bin/sh
 # Compile the reference's Tier-1 block decoder where it lies (no copies) together with
 # oracle/ref_t1_driver.cpp into oracle/_ref/libref_t1.so.  Needs the reference tree
-# (default /root/reference); the shared object is git-ignored and travels with the repo.
+# (argument or J2K_REFERENCE_DIR); the shared object is git-ignored and travels with the repo.
 set -e
-REF=${1:-/root/reference}
+REF=${1:-$J2K_REFERENCE_DIR}
+[ -n "$REF" ] || { echo "usage: $0 <reference root> (or set J2K_REFERENCE_DIR)" >&2; exit 2; }
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 D="$REF/decoder"

@@ -22,6 +22,8 @@
 #     oracle/ref_gpu_stub.c, which reports "no GPU"; the engine is run with mUsingGpu false.
 #   * the templates that decoderconcrete.cpp uses from bmi_cpu_dwt_decoder.cpp are
 #     instantiated by oracle/ref_cpu_dwt_unit.cpp, which compiles that file by #include.
+#   * the driver's operator new zero-fills (an uninitialised job-queue member otherwise hangs
+#     the engine at random on Linux; see oracle/ref_cpu_driver.cpp).
 set -e
 REF=${1:-$J2K_REFERENCE_DIR}
 [ -n "$REF" ] || { echo "usage: $0 <reference root> (or set J2K_REFERENCE_DIR)" >&2; exit 2; }
@@ -64,6 +66,6 @@ for s in $SRCS; do
   $CXX $INC -c "$s" -o "$o" 2> "$o.log" || { grep -v "obsolete option" "$o.log" >&2; echo "failed: $s" >&2; exit 1; }
   OBJS="$OBJS $o"
 done
-g++ -shared -o "$OUT/libref_cpu.so" $OBJS -lpthread
+g++ -shared -Wl,-Bsymbolic -o "$OUT/libref_cpu.so" $OBJS -lpthread
 rm -rf "$OBJ"
 echo "built $OUT/libref_cpu.so"

@@ -11,10 +11,29 @@
  * decoderconcrete.cpp:136-153).
  */
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #include <time.h>
 
+#include <new>
+
 #include "codec_base.h"
+
+/* Zero-filled heap for the reference's objects.  Its job queue leaves a member
+ * uninitialised outside Windows (SemaphoreControledJobQueue::mInited, initialised only under
+ * `#if _WINDOWS` in decoder/core/include/jobqueue.h), and Init (jobqueue.cpp:15-26) then
+ * skips creating its semaphore and mutex whenever the heap hands back non-zero memory: the
+ * engine hangs or aborts in pthread_mutex_lock at random.  Allocating zeroed memory, as a
+ * fresh heap gives, removes that without touching the reference's code.  The library is
+ * linked with -Bsymbolic so these replace operator new only inside it. */
+void *operator new(size_t n) throw(std::bad_alloc) {
+  void *p = calloc(1, n ? n : 1);
+  if (!p) throw std::bad_alloc();
+  return p;
+}
+void *operator new[](size_t n) throw(std::bad_alloc) { return operator new(n); }
+void operator delete(void *p) throw() { free(p); }
+void operator delete[](void *p) throw() { free(p); }
 
 namespace {
 bool g_inited = false;
