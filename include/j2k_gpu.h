@@ -172,7 +172,11 @@ int j2k_gpu_autotune(j2k_gpu_ctx *ctx, void *stream, int iters, j2k_gpu_tuning *
  * static device array of J2K_NOALLOC_SCRATCH_BYTES held by every GPU that loads the
  * library; tile-components needing more than that (2 * res_w[L-1] * res_h[L-1] * 4 bytes)
  * return J2K_ERR_UNSUPPORTED.  The first call on a device looks up the array's device
- * address (make it before any stream capture); overlapping calls race on the array.
+ * address (make it before any stream capture); the address is kept for the life of the
+ * process, so a caller that resets the device must restart the process before calling
+ * again.  Overlapping calls race on the array.  A resolution table that does not nest
+ * inside the tile-component returns J2K_ERR_ARG before anything is enqueued; a CUDA error
+ * already pending from earlier work returns J2K_ERR_CUDA and stays pending.
  * Asynchronous on `stream`. */
 #define J2K_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int j2k_gpu_tile_idwt_noalloc(const j2k_tilecomp *tc, int reversible, int flags, const void *coef, void *out,

@@ -12,10 +12,19 @@
  * holds it until the process exits.  In host code the array's name is only a host-side
  * stand-in, so its device address is fetched once per device with cudaGetSymbolAddress
  * (with that device current) on the first call there; make that first call before any
- * stream capture.  Calls share the array: calls that overlap on the GPU (different streams,
- * or devices reusing one process-wide lock-free entry) race and must be serialised by the
- * caller.  Nothing needs clearing between calls: every scratch element a level reads was
- * written by the previous level of the same call.
+ * stream capture.  The address is cached for the life of the process: after cudaDeviceReset
+ * (or anything else that tears down and re-creates a device's primary context) the cached
+ * address is stale, so such a caller must restart the process before calling again.  Calls
+ * share the array: calls that overlap on the GPU (different streams, or devices reusing one
+ * process-wide lock-free entry) race and must be serialised by the caller.  Nothing needs
+ * clearing between calls: every scratch element a level reads was written by the previous
+ * level of the same call.
+ *
+ * Errors: the tile-component description is checked before anything is enqueued (a table
+ * whose resolutions do not nest inside the tile-component returns J2K_ERR_ARG); a CUDA error
+ * already pending on the calling thread from earlier work is reported as J2K_ERR_CUDA and
+ * left pending for its owner; a failed launch of this call is cleared and reported as
+ * J2K_ERR_CUDA.
  */
 #include <cuda_runtime.h>
 
@@ -77,8 +86,27 @@ int run_levels(const j2k_tilecomp &tc, int flags, const void *coef, void *out, i
     j2k_dev::dwt_level_explicit_kernel<REV><<<tiles, j2k_dev::DWT_THREADS, 0, st>>>(reinterpret_cast<const T *>(coef), tc.w, llsrc,
                                                                    stride_ll, dst, stride_out, rw, rh, lw, lh,
                                                                    (!REV && r > 1) ? 1 : 0, llg, refc);
+    if (cudaPeekAtLastError() != cudaSuccess) {  // nothing was pending on entry: this error is ours
+      cudaGetLastError();
+      return J2K_ERR_CUDA;
+    }
   }
-  return cudaGetLastError() == cudaSuccess ? J2K_OK : J2K_ERR_CUDA;
+  return J2K_OK;
+}
+
+// Resolutions must nest: the full resolution is the tile-component, every coarser one lies
+// inside the next finer one and is half of it (rounded either way, as the band origin
+// decides).  Anything else would make the level kernels address outside the caller's buffers
+// or the scratch array.
+bool table_consistent(const j2k_tilecomp &tc) {
+  const int L = tc.levels;
+  if (tc.res_w[L] != tc.w || tc.res_h[L] != tc.h) return false;
+  for (int r = 0; r < L; ++r) {
+    const int w = tc.res_w[r], h = tc.res_h[r], fw = tc.res_w[r + 1], fh = tc.res_h[r + 1];
+    if (w < 0 || h < 0 || w > fw || h > fh) return false;
+    if (w < fw / 2 || w > (fw + 1) / 2 || h < fh / 2 || h > (fh + 1) / 2) return false;
+  }
+  return true;
 }
 
 }  // namespace
@@ -87,9 +115,11 @@ extern "C" int j2k_gpu_tile_idwt_noalloc(const j2k_tilecomp *tc, int reversible,
                                          int out_stride, void *stream) {
   if (!tc || !coef || !out || out_stride < tc->w || tc->w <= 0 || tc->h <= 0) return J2K_ERR_ARG;
   if (tc->levels < 0 || tc->levels > J2K_MAX_LEVELS) return J2K_ERR_ARG;
+  if (!table_consistent(*tc)) return J2K_ERR_ARG;
   const int L = tc->levels;
   const size_t need = L >= 2 ? 2 * (size_t)tc->res_w[L - 1] * tc->res_h[L - 1] * 4 : 0;
   if (need > kScratchBytes) return J2K_ERR_UNSUPPORTED;  // beyond the static scratch size
+  if (cudaPeekAtLastError() != cudaSuccess) return J2K_ERR_CUDA;  // earlier work's error: left for its owner
   cudaStream_t st = (cudaStream_t)stream;
   if (L == 0) {
     // no lifting: the coefficients are the samples

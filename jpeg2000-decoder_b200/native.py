@@ -30,6 +30,7 @@ FLAG_REF_COMPAT = 1
 FLAG_KEEP_COMPONENTS = 2
 
 J2K_OK = 0
+J2K_ERR_ARG = -1
 J2K_ERR_PARSE = -2
 J2K_ERR_NODEVICE = -9
 J2K_ERR_DECODE = -7

@@ -198,3 +198,30 @@ def test_no_cpu_fallback_without_device(pkg):
     with pytest.raises(native.J2kError) as e:
         native.Server()
     assert e.value.code == native.J2K_ERR_NODEVICE
+
+
+def test_noalloc_idwt_refuses_inconsistent_resolution_tables(pkg):
+    """The allocation-free inverse DWT checks a hand-built tile-component description
+    before it enqueues anything: resolutions that do not nest inside the tile-component (a
+    full resolution other than the tile size, a level larger than the next finer one, or
+    not half of it) return J2K_ERR_ARG.  No device is touched, so this runs on the CPU."""
+    import ctypes
+    from jpeg2000_decoder_b200 import native
+    fn = native.lib().j2k_gpu_tile_idwt_noalloc
+
+    def tc_with(res_w, res_h, w=64, h=48):
+        tc = native.TileComp()
+        tc.w, tc.h, tc.levels = w, h, len(res_w) - 1
+        for r, (a, b) in enumerate(zip(res_w, res_h)):
+            tc.res_w[r], tc.res_h[r] = a, b
+        return tc
+
+    bad_tables = [([16, 32, 65], [12, 24, 48]),    # full resolution wider than the tile-component
+                  ([16, 32, 64], [12, 24, 4096]),  # full resolution taller than the caller's buffer
+                  ([40, 32, 64], [12, 24, 48]),    # a coarser level wider than the next finer one
+                  ([16, 20, 64], [12, 24, 48]),    # a level that is not half of the next one
+                  ([-1, 32, 64], [12, 24, 48])]    # negative size
+    for res_w, res_h in bad_tables:
+        tc = tc_with(res_w, res_h)
+        rc = fn(ctypes.byref(tc), 1, 0, ctypes.c_void_p(16), ctypes.c_void_p(16), 64, None)
+        assert rc == native.J2K_ERR_ARG, (res_w, res_h, rc)
