@@ -1,6 +1,7 @@
 """Throughput benchmark of the B200 JPEG 2000 Part-1 decode path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3|c2|c4|c1|c5] [--impl ours|reference]
+    python bench.py --workload c3 --frames 16 --decode-repeat 2 [--t1-form 1]   (profiling mode)
 
 Default workload (metric: Mpixel/s decoded, batched): the batched video-frame decode —
 64 frames of 1920x1080 RGB 8-bit, 9/7 + ICT, 512x512 tiles, 5 levels, 64x64 code-blocks,
@@ -136,65 +137,196 @@ def replica_throughput(units_per_rank, world, steps, total_time_s):
     return units_per_rank * world * steps / total_time_s
 
 
-# ------------------------------------------------------------------ CPU (oracle) -------
+# ------------------------------------------------------------------ CPU baselines -------
+def reference_sample(name, streams):
+    """Codestreams of this workload that the reference's own decoder takes, and what they are.
+
+    C1, C2 and the serving requests are single-tile pictures it decodes (bit-exact against
+    ours, tests/test_cpu_reference_pictures.py).  It segfaults on C3's frames (their partial
+    512x512 edge tiles), so C3 is sampled by the same coding parameters on the 3 x 2 full
+    tiles of C3 frames.  Its Tier-1 has no BYPASS / RESET (bmi_mq_decoder.cpp:206-210), so C4
+    has no reference sample."""
+    if name == "c3":
+        frames = synth.video_frames(3, n=4)
+        cs = [native.encode(np.ascontiguousarray(f[:, :1024, :1536]), 8, **synth.C3_PARAMS) for f in frames]
+        return cs, ("C3 coding parameters (9/7+ICT, 512x512 tiles, 3 layers) on the 3x2 full tiles (1536x1024) of "
+                    "4 C3 frames; the reference's decoder segfaults on C3's partial edge tiles")
+    if name in ("c1", "c2"):
+        return list(streams[:1]), "the workload's picture"
+    if name == "c5":
+        return list(streams), "the %d distinct requests of the serving pool" % len(streams)
+    return None, "no reference sample: the reference's Tier-1 implements no BYPASS / RESET"
+
+
+def reference_cpu(name, streams, fmt, steps, warmup, workers=None, step_seconds=1.0, per_process=20):
+    """The reference's own CPU decoder (BMI::Decoder built from its sources into
+    oracle/_ref/libref_cpu.so; oracle/ref_cpu_runner.py runs it in child processes) on the
+    workload's reference sample, on every host core.
+
+    The reference engine's worker threads race: with several workers per engine it stops
+    after a few dozen decodes (a picture whose status never leaves PARSING, or a segfault),
+    while single-worker engines decode reliably.  So the host's cores each run their own
+    single-worker engine process (EnginConfig::mThreadNum = 1), each decoding one sample
+    picture over and over (pictures assigned round-robin), at most `per_process` timed
+    decodes per process after one untimed decode of its own; each decode is timed inside
+    its process as the wall clock of Decode() + GetResult() (the reference's Tier-2
+    included).  One step = `passes` decodes per process, as many as fill about
+    `step_seconds`; a step lasts as long as its slowest process.  None when the library
+    or a sample is missing."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_cpu_runner
+    if not ref_cpu_runner.available():
+        return None
+    cs, what = reference_sample(name, streams)
+    if not cs:
+        return None
+    workers = workers or os.cpu_count() or 1
+    fmts = [fmt if fmt is not None else synth.c5_format(c) for c in cs]
+
+    def timed(i, n):
+        """n timed decodes of sample picture i on a single-worker engine: ms each, size."""
+        out, size = [], None
+        while len(out) < n:
+            k = min(per_process, n - len(out))
+            r = ref_cpu_runner.decode([cs[i]], fmts[i], threads=1, reps=k + 1, timeout=600, time_only=True)
+            if not r["ok"]:
+                raise RuntimeError(r["error"])
+            out += r["ms"][0][1:]
+            size = r["sizes"][0]
+        return out, size
+
+    try:
+        one_ms = max(timed(i, 1)[0][0] for i in range(len(cs)))
+        passes = max(1, int(round(step_seconds * 1e3 / max(one_ms, 1e-3))))
+        n = (warmup + steps) * passes
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            runs = list(ex.map(lambda w: timed(w % len(cs), n), range(workers)))
+    except RuntimeError as e:
+        return {"error": str(e)}
+    step_ms = [max(sum(ms[(warmup + k) * passes:(warmup + k + 1) * passes]) for ms, _ in runs) for k in range(steps)]
+    px = sum(w * h for _, (w, h) in runs) * passes * steps
+    total_s = sum(step_ms) / 1e3
+    return {"value": px / total_s / 1e6, "unit": "Mpixel/s", "cores": workers, "kind": "reference",
+            "sample": "%s; %d single-worker reference engines (one per host core) each decoding %d pictures per "
+                      "step, %d timed steps after %d warm-up steps, %.1f s" % (
+                          what, workers, passes, steps, warmup, total_s),
+            "ms_per_step": total_s * 1e3 / steps}
+
+
 def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
-    """Decode a bounded sample of the workload with the CPU restatement on all host cores."""
+    """The CPU restatement of the reference's path (oracle/liboracle.so) on a bounded sample
+    of the workload: one picture per host thread at a time (host Tier-2 of each picture
+    inside the timed loop); `cores` is the number of threads that had a picture."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from jpeg2000_decoder_b200 import build
-    build.build_oracle(reference="/nonexistent")
+    build.build_oracle()
     import oracle_util
     threads = threads or os.cpu_count() or 1
-    plans = [native.Plan(s) for s in streams[:max(1, min(len(streams), threads))]]
+    sample = list(streams[:max(1, min(len(streams), threads))])
+    used = min(len(sample), threads)
 
-    def one(p):
+    def one(cs):
+        p = native.Plan(cs)
         f = fmt if fmt is not None else (native.FMT_24BITS_RGB if p.info.bitdepth <= 8 else native.FMT_48BITS_RGB)
         oracle_util.oracle_decode(p, f)
         return p.info.width * p.info.height
 
     orc = oracle_util.orc()
     orc.oracle_decisions.restype = ctypes.c_ulonglong
-    with ThreadPoolExecutor(max_workers=threads) as ex:
+    with ThreadPoolExecutor(max_workers=used) as ex:
         d0 = orc.oracle_decisions()
         t0 = time.perf_counter()
         px = 0
         rounds = 0
         while True:
-            px += sum(ex.map(one, plans))
+            px += sum(ex.map(one, sample))
             rounds += 1
             if time.perf_counter() - t0 > budget_s or rounds >= 8:
                 break
         dt = time.perf_counter() - t0
         decisions_per_px = (orc.oracle_decisions() - d0) / max(1, px)
     cpu_decode_sample.decisions_per_px = decisions_per_px
-    return px / dt / 1e6, threads, "%d image decodes (%d distinct) in %.1f s" % (rounds * len(plans), len(plans), dt)
+    return {"value": px / dt / 1e6, "unit": "Mpixel/s", "cores": used, "kind": "port",
+            "sample": "%d picture decodes (%d distinct, host Tier-2 included) in %.1f s on %d threads" % (
+                rounds * len(sample), len(sample), dt, used)}
 
 
 cpu_decode_sample.decisions_per_px = None
+
+
+def cpu_baseline(name, streams, fmt, steps=10, warmup=2, port_budget=8.0):
+    """The reference where it decodes the workload, else the CPU restatement; the port's
+    figure rides along, so the reader can scale one by the other."""
+    ref = reference_cpu(name, streams, fmt, steps, warmup, step_seconds=1.0)
+    port = cpu_decode_sample(streams, fmt, budget_s=port_budget)
+    if ref and "error" not in ref:
+        out = dict(ref)
+        out["port"] = {k: (round(v, 3) if isinstance(v, float) else v) for k, v in port.items()}
+        return out
+    out = dict(port)
+    if ref:
+        out["reference_error"] = ref["error"]
+    return out
 
 
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
     cfg, streams, fmt = workload(args.workload, args.quick)
-    for _ in range(args.warmup):
-        cpu_decode_sample(streams, fmt, budget_s=1.0)
-    vals = []
-    sample = ""
-    cores = os.cpu_count()
-    for _ in range(args.steps):
-        v, cores, sample = cpu_decode_sample(streams, fmt, budget_s=5.0)
-        vals.append(v)
-    value = float(np.median(vals))
+    base = reference_cpu(args.workload, streams, fmt, args.steps, args.warmup)
+    if not base or "error" in base:
+        port = [cpu_decode_sample(streams, fmt, budget_s=1.0) for _ in range(args.warmup)]
+        port = [cpu_decode_sample(streams, fmt, budget_s=5.0) for _ in range(args.steps)]
+        reason = base["error"] if base else reference_sample(args.workload, streams)[1]
+        base = dict(port[-1], value=float(np.median([p["value"] for p in port])), reference_unavailable=reason)
+    value = base["value"]
     line = {"metric": METRIC, "value": round(value, 3), "unit": "Mpixel/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/int32", "data": "synthetic (seeded, project encoder)", "config": cfg, "impl": "reference",
-            "cpu_baseline": {"value": round(value, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in base.items()},
             "e2e": {"value": round(value, 3), "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
 # ------------------------------------------------------------------ GPU arm -----------
+def fp64_check(ctx, plans, fmt, frames=2):
+    """PSNR and max-abs of the device's packed 9/7 pictures against an FP64 T.800
+    synthesis (tests/fp64_97.py) of the device's own Tier-1 values, on the first `frames`
+    pictures of the batch.  Each block's Tier-1 values are its stage-0 coefficients divided
+    by the block's gain (exact to float32 rounding, ~1e-7 relative), so the comparison
+    measures the FP32 dequantisation, lifting, ICT and (int) truncation only."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import fp64_97
+    worst_psnr, worst_abs = float("inf"), 0.0
+    for p in plans[:frames]:
+        ctx.begin()
+        slot = ctx.add(p, fmt)  # the benched path: last level fused with the ICT and pack
+        ctx.launch()
+        assert ctx.sync() == 0
+        coef = ctx.coefficients(slot, 0).astype(np.float64)
+        out = ctx.output(slot)
+
+        def raw(i, cb, coef=coef):
+            v = np.empty((cb.h, cb.w))
+            for y in range(cb.h):
+                o = cb.out_off + y * cb.out_stride
+                v[y] = coef[o:o + cb.w] / cb.gain
+            return v
+        want = fp64_97.synthesize(p, raw)
+        I = p.info
+        if fmt == native.FMT_24BITS_RGB:
+            got = out.reshape(I.height, I.width, 3)[:, :, [2, 1, 0]].transpose(2, 0, 1)
+        elif fmt == native.FMT_48BITS_RGB:
+            got = out.view(np.uint16).reshape(I.height, I.width, 3)[:, :, [2, 1, 0]].transpose(2, 0, 1) >> (
+                16 - I.bitdepth)
+        else:
+            return None
+        ps, mx = fp64_97.psnr_maxabs(got, want, I.bitdepth)
+        worst_psnr, worst_abs = min(worst_psnr, ps), max(worst_abs, mx)
+    return {"pictures": min(frames, len(plans)), "psnr_db_min": round(worst_psnr, 2), "max_abs": round(worst_abs, 3),
+            "against": "FP64 T.800 dequantisation + 9/7 synthesis + ICT of the same Tier-1 values, before rounding"}
+
+
 def run_gpu(args, rank, world, dist):
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -315,6 +447,18 @@ def run_gpu(args, rank, world, dist):
     e2e_ms = [e2e_s * 1e3 / n_e2e]
     ctx2.close()
 
+    # ---- PSNR / max-abs of the FP32 9/7 path against an FP64 synthesis of the same Tier-1
+    fp64 = fp64_check(ctx, plans, fmt) if not plans[0].info.reversible and not args.no_fp64 else None
+
+    # ---- a shortened serving stream (C5 mix) through the continuous-batching service
+    serving = None
+    if args.workload != "c5" and not args.no_serving:
+        _, spool, _ = workload("c5", True)
+        m = serve_measure(dev, spool, args.serving_requests, args.depth, args.batch_mpix, 0.0, 1, 5 + rank, dist)
+        _, serving = serving_summary(m, world)
+        serving["stream"] = "C5 mix: %d requests drawn from %d distinct seeded requests" % (
+            args.serving_requests, len(spool))
+
     if rank != 0:
         return
     # ---- roofline of the dominant kernel (Tier-1) and of the DWT + MCT stage
@@ -336,7 +480,7 @@ def run_gpu(args, rank, world, dist):
                 "frac": round(dwt_bytes / (dwt_ms / 1e3) / 1e9 / peak, 4), "traffic": tr.get("dwt_bytes_per_step"),
                 "kernel": "dwt_level_kernel + output_kernel", "peak_source": peak_kind,
                 "algorithmic_bytes": dwt_bytes, "ms_per_step": round(dwt_ms, 4)}
-    cpu_v, cores, sample = cpu_decode_sample(streams, fmt, budget_s=args.cpu_budget)
+    base = cpu_baseline(args.workload, streams, fmt, port_budget=args.cpu_budget)
     dpp = cpu_decode_sample.decisions_per_px
     if dpp:
         # Tier-1 work rate: decisions of the standard decoding process (MQ symbols incl. run
@@ -376,38 +520,38 @@ def run_gpu(args, rank, world, dist):
                     "host_ms_per_step": {k: round(v / n_e2e, 3) for k, v in host_ms.items()}},
             "plain_gpu_path": {"value": round(plain, 2), "unit": "Mpixel/s", "images": len(uniq),
                                "what": "one image per launch sequence, host buffers"},
-            "speedup_vs_plain": round(value / plain, 2),
+            "speedup_vs_plain": round(e2e / plain, 2),
+            "speedup_vs_plain_note": "e2e / plain_gpu_path: both host buffer to host buffer, wall clock",
             "roofline": roof_t1 if dominant == "t1" else roof_dwt,
             "roofline_dwt": roof_dwt, "roofline_t1": roof_t1, "roofline_t1_issue": roof_t1_issue,
             "stage_ms": {"t1": round(t1_ms, 4), "dwt_mct": round(dwt_ms, 4)},
-            "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
-                             "sample": sample},
+            "cpu_baseline": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in base.items()},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks}
+    if fp64:
+        line["config"]["fp64_check"] = fp64
+    if serving:
+        line["serving"] = serving
     print(json.dumps(line))
 
 
 # ------------------------------------------------------------------ serving (C5) -------
-def run_serve(args, rank, world, dist):
-    """C5: requests of mixed size / depth / wavelet through the continuous-batching service.
+def serve_measure(dev, pool, n_req, depth, batch_mpix, rate=0.0, warmup=1, seed=5, dist=None, sampler=None):
+    """Requests of mixed size / depth / wavelet through the continuous-batching service.
 
     Phase 1 (throughput): the whole request stream is submitted at once from several
-    threads while client threads take and release each result; value = decoded Mpixel/s
-    over that wall time (codestreams in host memory, packed pixels back in host memory: an
-    end-to-end figure).  Phase 2 (latency):
-    Poisson arrivals at `--rate` requests/s (default 70% of the phase-1 request rate);
-    p50 / p99 are submit-to-result times.  The plain path decodes the same stream one
-    request per launch sequence on one context."""
+    threads while client threads take and release each result; Mpixel/s over that wall time
+    (codestreams in host memory, packed pixels back in host memory: an end-to-end figure).
+    Phase 2 (latency): Poisson arrivals at `rate` requests/s (default 70 % of the phase-1
+    request rate); p50 / p99 are submit-to-result times.  The plain path decodes the same
+    stream one request per launch sequence on one context, also host buffer to host buffer,
+    so plain and served are measured the same way."""
     import threading
 
     import torch
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(dev)
-    cfg, pool, _ = workload("c5", args.quick)
     fmts = [synth.c5_format(cs) for cs in pool]
     px_of = [native.Plan(cs).info.width * native.Plan(cs).info.height for cs in pool]
-    n_req = args.requests or (200 if args.quick else 2000)
-    rng = np.random.default_rng(5 + rank)
+    rng = np.random.default_rng(seed)
     order = [int(i) for i in rng.integers(0, len(pool), n_req)]
     total_px = sum(px_of[i] for i in order)
 
@@ -424,7 +568,7 @@ def run_serve(args, rank, world, dist):
     plain = sum(px_of[i] for i in order[:n_plain]) / plain_s / 1e6
     ctx.close()
 
-    srv = native.Server(device=dev, pipeline_depth=args.depth, max_batch_pixels=int(args.batch_mpix * 2 ** 20))
+    srv = native.Server(device=dev, pipeline_depth=depth, max_batch_pixels=int(batch_mpix * 2 ** 20))
 
     def serve_pass(idx, when=None):
         """Submit idx (at times `when` after the start, else at once) from 8 threads while 4
@@ -461,7 +605,7 @@ def run_serve(args, rank, world, dist):
         return time.perf_counter() - t_start, failed[0]
 
     # ---- warm-up: the device pools and pinned buffers grow to their steady-state sizes
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         serve_pass(order)
 
     # ---- phase 1: saturation
@@ -469,56 +613,108 @@ def run_serve(args, rank, world, dist):
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
-        sat_s, bad = serve_pass(order)
-        torch.cuda.synchronize()
+    if sampler:
+        sampler.__enter__()
+    sat_s, bad = serve_pass(order)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.__exit__()
     st1 = srv.stats()
     sat_s = max_over_ranks(sat_s, dist)
-    value = replica_throughput(total_px, world, 1, sat_s) / 1e6
 
     # ---- phase 2: Poisson arrivals
-    rate = args.rate or 0.7 * n_req / sat_s
+    rate = rate or 0.7 * n_req / sat_s
     gaps = rng.exponential(1.0 / rate, n_req)
     when = np.cumsum(gaps) - gaps[0]
     srv.reset_stats()
     poisson_s, bad2 = serve_pass(order, when)
-    bad += bad2
     st2 = srv.stats()
     srv.close()
+    return {"order": order, "fmts": fmts, "total_px": total_px, "sat_s": sat_s, "bad": bad + bad2, "plain": plain,
+            "n_plain": n_plain, "st1": st1, "st2": st2, "rate": rate, "poisson_s": poisson_s}
+
+
+def serving_summary(m, world):
+    n_req = len(m["order"])
+    value = replica_throughput(m["total_px"], world, 1, m["sat_s"]) / 1e6
+    st1, st2 = m["st1"], m["st2"]
+    return value, {
+        "saturation": {"mpix_s": round(value, 2), "requests_s": round(n_req / m["sat_s"], 1),
+                       "gpu_busy_ms": round(st1["gpu_ms"], 2), "wall_ms": round(m["sat_s"] * 1e3, 2),
+                       "host_stage_ms": round(st1["stage_ms"], 2), "host_enqueue_ms": round(st1["enqueue_ms"], 2),
+                       "pool_growths": st1["pool_growths"], "pinned_allocs": st1["pinned_allocs"],
+                       "batches": st1["batches"], "mean_batch_images": round(st1["mean_batch_images"], 2),
+                       "p50_ms": round(st1["p50_us"] / 1e3, 3), "p99_ms": round(st1["p99_us"] / 1e3, 3)},
+        "poisson": {"rate_rps": round(m["rate"], 1),
+                    "offered_mpix_s": round(m["rate"] * m["total_px"] / n_req / 1e6, 1),
+                    "achieved_mpix_s": round(m["total_px"] / m["poisson_s"] / 1e6, 2),
+                    "p50_ms": round(st2["p50_us"] / 1e3, 3), "p99_ms": round(st2["p99_us"] / 1e3, 3),
+                    "max_ms": round(st2["max_us"] / 1e3, 3), "batches": st2["batches"],
+                    "mean_batch_images": round(st2["mean_batch_images"], 2)},
+        "plain_gpu_path": {"mpix_s": round(m["plain"], 2), "requests": m["n_plain"],
+                           "what": "one request per launch sequence, host buffer to host buffer"},
+        "served_vs_plain": round(value / m["plain"], 2), "requests": n_req, "bad_requests": m["bad"]}
+
+
+def run_serve(args, rank, world, dist):
+    """C5: the serving stream (serve_measure) as the bench line."""
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg, pool, _ = workload("c5", args.quick)
+    n_req = args.requests or (200 if args.quick else 2000)
+    clk = ClockSampler(dev)
+    m = serve_measure(dev, pool, n_req, args.depth, args.batch_mpix, args.rate, args.warmup, 5 + rank, dist, clk)
     if rank != 0:
         return
-    cpu_v, cores, sample = cpu_decode_sample(pool, None, budget_s=args.cpu_budget)
+    value, serving = serving_summary(m, world)
+    base = cpu_baseline("c5", pool, None, port_budget=args.cpu_budget)
+    order, fmts = m["order"], m["fmts"]
     h2d = sum(len(pool[i]) for i in order)
     cfg = dict(cfg)
-    cfg.update({"requests": n_req, "pipeline_depth": args.depth, "batch_mpix_cap": args.batch_mpix, "parallelism": "replicas x%d" % world,
-                "bad_requests": bad, "l2": "inputs differ per request; no flush"})
+    cfg.update({"requests": n_req, "pipeline_depth": args.depth, "batch_mpix_cap": args.batch_mpix,
+                "parallelism": "replicas x%d" % world, "bad_requests": m["bad"],
+                "l2": "inputs differ per request; no flush"})
     line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": 1,
-            "warmup": args.warmup, "ms_per_step": round(sat_s * 1e3, 3), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": round(m["sat_s"] * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (9/7) / int32 (5/3)",
             "data": "synthetic (seeded requests, project encoder)", "config": cfg,
             "e2e": {"value": round(value, 2), "unit": "Mpixel/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(sum(native.Plan(pool[i]).output_bytes(fmts[i]) for i in order)),
                     "includes": "submit (host Tier-2) + merged batches + D2H of every request, wall clock"},
-            "serving": {"saturation": {"mpix_s": round(value, 2), "requests_s": round(n_req / sat_s, 1),
-                                       "gpu_busy_ms": round(st1["gpu_ms"], 2), "wall_ms": round(sat_s * 1e3, 2),
-                                       "host_stage_ms": round(st1["stage_ms"], 2),
-                                       "host_enqueue_ms": round(st1["enqueue_ms"], 2),
-                                       "pool_growths": st1["pool_growths"], "pinned_allocs": st1["pinned_allocs"],
-                                       "batches": st1["batches"], "mean_batch_images": round(st1["mean_batch_images"], 2),
-                                       "p50_ms": round(st1["p50_us"] / 1e3, 3), "p99_ms": round(st1["p99_us"] / 1e3, 3)},
-                        "poisson": {"rate_rps": round(rate, 1), "offered_mpix_s": round(rate * total_px / n_req / 1e6, 1),
-                                    "achieved_mpix_s": round(total_px / poisson_s / 1e6, 2),
-                                    "p50_ms": round(st2["p50_us"] / 1e3, 3), "p99_ms": round(st2["p99_us"] / 1e3, 3),
-                                    "max_ms": round(st2["max_us"] / 1e3, 3), "batches": st2["batches"],
-                                    "mean_batch_images": round(st2["mean_batch_images"], 2)}},
-            "plain_gpu_path": {"value": round(plain, 2), "unit": "Mpixel/s", "requests": n_plain,
-                               "what": "one request per launch sequence, host buffers"},
-            "speedup_vs_plain": round(value / plain, 2),
-            "cpu_baseline": {"value": round(cpu_v, 3), "unit": "Mpixel/s", "cores": cores, "kind": "port",
-                             "sample": sample},
-            "gpu_launches": int(st1["launches"]),
+            "serving": serving,
+            "plain_gpu_path": {"value": serving["plain_gpu_path"]["mpix_s"], "unit": "Mpixel/s",
+                               "requests": m["n_plain"], "what": "one request per launch sequence, host buffers"},
+            "speedup_vs_plain": serving["served_vs_plain"],
+            "cpu_baseline": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in base.items()},
+            "gpu_launches": int(m["st1"]["launches"]),
             "clocks": clk.summary()}
     print(json.dumps(line))
+
+
+def run_decode_repeat(args):
+    """Profiling mode: decode the workload (or its first --frames pictures) --decode-repeat
+    times, one batch decode each, printing the stage times; no bench line.  Run it under
+    ncu with -s / -c to capture a chosen launch of a chosen kernel."""
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    cfg, streams, fmt = workload(args.workload, args.quick)
+    if args.frames > 0:
+        streams = streams[:args.frames]
+    ctx = native.GpuContext(dev)
+    ctx.set_tuning(t1_form=args.t1_form)
+    plans = [native.Plan(s) for s in streams]
+    for it in range(args.decode_repeat):
+        ctx.begin()
+        for p in plans:
+            ctx.add(p, fmt)
+        ctx.launch()
+        rc = ctx.sync()
+        if rc != 0:
+            raise SystemExit("decode failed: %d" % rc)
+        print(args.workload, it, ctx.timing(), "launches", ctx.launches(), flush=True)
+    ctx.close()
 
 
 def main():
@@ -536,12 +732,22 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-autotune", action="store_true", help="skip the Tier-1 shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="enqueue launches instead of replaying a CUDA graph")
+    ap.add_argument("--no-serving", action="store_true", help="skip the shortened serving stream of the default line")
+    ap.add_argument("--serving-requests", type=int, default=240, help="requests of the shortened serving stream")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error check")
+    ap.add_argument("--decode-repeat", type=int, default=0,
+                    help="profiling mode: decode the workload this many times, print stage times, no bench line")
+    ap.add_argument("--frames", type=int, default=0, help="profiling mode: only the first N pictures")
+    ap.add_argument("--t1-form", type=int, default=0, help="profiling mode: Tier-1 form 0 auto, 1 compact, 2 unrolled")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
     if args.impl == "reference":
         run_reference_arm(args, rank, world)
+        return
+    if args.decode_repeat:
+        run_decode_repeat(args)
         return
     if world > 1:
         import datetime
