@@ -21,6 +21,10 @@ void bmi_decoder_set_job(int output_format, int dwt_top_level, unsigned ignore_c
 int bmi_decoder_decode(const void *buf, int size, double *ms);
 /* Decoder::PreDecode(): returns a BMI::Status, fills the main-header properties. */
 int bmi_decoder_predecode(const void *buf, int size, int *width, int *height, int *ncomp, int *bitdepth, int *levels);
+/* Decoder::PreDecode() as above, reporting CodeStreamProperties::mFormat (EncodeFormat: RAW,
+ * RGB, YUV444, YUV422, YUV420, BAYERGRB, COMPONENT4; from the component sampling and the
+ * JP2 colour space, dec_jp2.cpp:488-523) and mMethod (0 = 5/3, 1 = 9/7).  Host only. */
+int bmi_decoder_predecode_format(const void *buf, int size, int *format, int *method);
 /* Decoder::CheckStatus() */
 int bmi_decoder_status(int handler);
 /* Decoder::GetResult() / GetThumbnail() / GetDecodedComponentInt() / GetDecodedComponentFloat() */

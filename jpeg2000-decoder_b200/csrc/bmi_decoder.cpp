@@ -44,6 +44,7 @@ struct Slot {
   int comp_loaded = -1;
   bool pending = false;
   int gpu_slot = -1;
+  int comp_w[J2K_MAX_COMPONENTS] = {0}, comp_h[J2K_MAX_COMPONENTS] = {0};  // each component's own grid
 };
 
 int fmt_bytes(int fmt) {
@@ -58,6 +59,25 @@ int fmt_bytes(int fmt) {
     case IMAGE_FOTMAT_64BITS_ARGB: return 8;
     default: return 0;
   }
+}
+
+// The reference's picture format (dec_jp2.cpp:488-523): from the component count, the
+// component sampling and, for three equally sampled components, the JP2 colour space (16
+// sRGB, 18 sYCC) or else the COD transform flag
+EncodeFormat encode_format(const j2k::StreamHeader &H) {
+  auto sub = [&](const int (&s)[J2K_MAX_COMPONENTS], int a, int b, int c) {
+    return s[0] == a && s[1] == b && s[2] == c;
+  };
+  if (H.ncomp == 1) return H.sub_x[0] == 1 && H.sub_y[0] == 1 ? RAW : UNKNOWN_FORMAT;
+  if (H.ncomp == 4) return COMPONENT4;
+  if (H.ncomp != 3) return UNKNOWN_FORMAT;
+  if (sub(H.sub_x, 1, 2, 2) && sub(H.sub_y, 1, 2, 2)) return YUV420;
+  if (sub(H.sub_x, 1, 2, 2) && sub(H.sub_y, 1, 1, 1)) return YUV422;
+  if (sub(H.sub_x, 1, 1, 1) && sub(H.sub_y, 1, 2, 2)) return BAYERGRB;
+  if (!sub(H.sub_x, 1, 1, 1) || !sub(H.sub_y, 1, 1, 1)) return UNKNOWN_FORMAT;
+  if (H.jp2_colr_method == 1 && H.jp2_colr_enum == 16) return RGB;
+  if (H.jp2_colr_method == 1 && H.jp2_colr_enum == 18) return YUV444;
+  return H.mct ? RGB : YUV444;
 }
 
 void fill_props(const j2k::StreamHeader &H, int discard, CodeStreamProperties &P, OutputFormat fmt) {
@@ -81,7 +101,7 @@ void fill_props(const j2k::StreamHeader &H, int discard, CodeStreamProperties &P
   P.mLayer = (short)H.layers;
   P.mBitDepth = (short)H.depth[0];
   P.mRoiShift = (short)H.roi_shift[0];
-  P.mFormat = H.ncomp == 1 ? RAW : (H.ncomp == 3 ? RGB : (H.ncomp == 4 ? COMPONENT4 : UNKNOWN_FORMAT));
+  P.mFormat = encode_format(H);
   P.mMethod = H.reversible[0] ? Ckernels_W5X3 : Ckernels_W9X7;
   P.mProgression = (Jp2_Progression)H.progression;
   P.mHeaderLength = (int)H.header_len;
@@ -159,6 +179,10 @@ class GpuDecoder : public Decoder {
     }
     const int discard = discard_of(H);
     fill_props(H, discard, s.props, s.cfg.mOutputFormat);
+    for (int c = 0; c < H.ncomp && c < J2K_MAX_COMPONENTS; ++c) {
+      s.comp_w[c] = H.comp_w(c, discard);
+      s.comp_h[c] = H.comp_h(c, discard);
+    }
     j2k_plan *plan = nullptr;
     int rc = j2k_plan_create_mt(s.codestream.data(), s.codestream.size(), discard, 0, s.cfg.mIgnoreComponents, tier2_threads(),
                                 &plan);
@@ -348,7 +372,8 @@ class GpuDecoder : public Decoder {
       return true;
     };
     if (resident_ != s.handler && !redecode()) return false;
-    const size_t n = (size_t)s.props.mOutputSize.x * s.props.mOutputSize.y;
+    // the component on its own grid: sub-sampled components are smaller than the picture
+    const size_t n = (size_t)s.comp_w[comp] * s.comp_h[comp];
     void *dst;
     if (s.props.mMethod == Ckernels_W5X3) {
       s.comp_int.resize(n);
@@ -437,6 +462,15 @@ int bmi_decoder_predecode(const void *buf, int size, int *width, int *height, in
     if (ncomp) *ncomp = p.mComponentNum;
     if (bitdepth) *bitdepth = p.mBitDepth;
     if (levels) *levels = p.mDwtLevel;
+  }
+  return (int)s;
+}
+int bmi_decoder_predecode_format(const void *buf, int size, int *format, int *method) {
+  BMI::CodeStreamProperties p;
+  BMI::Status s = BMI::Decoder::Get()->PreDecode(buf, size, p);
+  if (s == BMI::READY) {
+    if (format) *format = (int)p.mFormat;
+    if (method) *method = (int)p.mMethod;
   }
   return (int)s;
 }

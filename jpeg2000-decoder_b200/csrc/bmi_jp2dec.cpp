@@ -78,14 +78,16 @@ int decode_planes(stru_dec_param *p, void *output[MAX_COMPONENT], int discard) {
         }
       }
     } else {
+      // each plane on its component's own grid (sub-sampled components are smaller)
       std::vector<int32_t> tmp(n);
       for (int comp = 0; comp < I.ncomp && comp < MAX_COMPONENT && rc == 0; ++comp) {
         if (!output[comp]) continue;
-        if (j2k_gpu_component_copy(c, 0, comp, tmp.data(), n * 4) != J2K_OK) {
+        const size_t nc = (size_t)I.comp_w[comp] * I.comp_h[comp];
+        if (j2k_gpu_component_copy(c, 0, comp, tmp.data(), nc * 4) != J2K_OK) {
           rc = -1;
           break;
         }
-        for (size_t i = 0; i < n; ++i) {
+        for (size_t i = 0; i < nc; ++i) {
           int v = I.reversible ? tmp[i] : (int)reinterpret_cast<const float *>(tmp.data())[i];
           v += dc;
           v = v < 0 ? 0 : (v > maxv ? maxv : v);

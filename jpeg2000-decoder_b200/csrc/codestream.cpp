@@ -29,6 +29,7 @@ namespace j2k {
 namespace {
 
 inline int ceil_div_pow2(int a, int l) { return (int)(((int64_t)a + (1LL << l) - 1) >> l); }
+inline int ceil_div(int a, int b) { return (int)(((int64_t)a + b - 1) / b); }
 inline int floor_log2(uint32_t v) { return v ? 31 - __builtin_clz(v) : -1; }
 
 struct Reader {
@@ -288,29 +289,60 @@ float irrev_ll_gain() {
   return g;
 }
 
-static size_t find_codestream(const uint8_t *d, size_t len) {
-  // JP2 wrapper: walk boxes to the contiguous codestream box 'jp2c'
-  if (len >= 12 && d[0] == 0 && d[1] == 0 && d[2] == 0 && d[3] == 12 && d[4] == 'j' && d[5] == 'P') {
-    size_t pos = 0;
-    while (pos + 8 <= len) {
-      uint64_t lbox = ((uint32_t)d[pos] << 24) | ((uint32_t)d[pos + 1] << 16) | ((uint32_t)d[pos + 2] << 8) | d[pos + 3];
-      uint32_t tbox = ((uint32_t)d[pos + 4] << 24) | ((uint32_t)d[pos + 5] << 16) | ((uint32_t)d[pos + 6] << 8) | d[pos + 7];
-      size_t hdr = 8;
-      if (lbox == 1) {
-        if (pos + 16 > len) return (size_t)-1;
-        lbox = 0;
-        for (int i = 0; i < 8; ++i) lbox = (lbox << 8) | d[pos + 8 + i];
-        hdr = 16;
-      } else if (lbox == 0) {
-        lbox = len - pos;
-      }
-      if (tbox == 0x6A703263) return pos + hdr;  // 'jp2c'
-      if (lbox < hdr) return (size_t)-1;
-      pos += lbox;
+// JP2 file format (T.800 Annex I): walk the boxes to the contiguous codestream box 'jp2c',
+// reading the colour specification of the header box on the way.  Mirrors the reference's
+// dec_read_jp2_header (dec_syntax.cpp:38-133): the signature and file-type boxes come first,
+// the header box (with ihdr / bpcc / colr / pclr / cmap / cdef / res) before 'jp2c', and the
+// colour specification's method and enumerated colour space are kept.  Unlike the reference,
+// boxes it does not know are skipped rather than refused (T.800 I.4).  Returns the offset of
+// the codestream, 0 for a bare codestream, (size_t)-1 for a malformed wrapper.
+static size_t find_codestream(const uint8_t *d, size_t len, StreamHeader &H) {
+  if (!(len >= 12 && d[0] == 0 && d[1] == 0 && d[2] == 0 && d[3] == 12 && d[4] == 'j' && d[5] == 'P')) return 0;
+  auto be32 = [&](size_t at) -> uint32_t {
+    return ((uint32_t)d[at] << 24) | ((uint32_t)d[at + 1] << 16) | ((uint32_t)d[at + 2] << 8) | d[at + 3];
+  };
+  // one box header at `pos` of [pos, limit): content start and end
+  auto box = [&](size_t pos, size_t limit, uint32_t &type, size_t &body, size_t &next) -> bool {
+    if (pos + 8 > limit) return false;
+    uint64_t lbox = be32(pos);
+    type = be32(pos + 4);
+    size_t hdr = 8;
+    if (lbox == 1) {
+      if (pos + 16 > limit) return false;
+      lbox = ((uint64_t)be32(pos + 8) << 32) | be32(pos + 12);
+      hdr = 16;
+    } else if (lbox == 0) {
+      lbox = limit - pos;
     }
-    return (size_t)-1;
+    if (lbox < hdr || lbox > limit - pos) return false;
+    body = pos + hdr;
+    next = pos + (size_t)lbox;
+    return true;
+  };
+  bool ftyp = false, jp2h = false;
+  size_t pos = 0;
+  for (;;) {
+    uint32_t type;
+    size_t body, next;
+    if (!box(pos, len, type, body, next)) return (size_t)-1;
+    if (type == 0x6A703263) return jp2h ? body : (size_t)-1;  // 'jp2c' after the header box
+    if (type == 0x66747970) ftyp = true;                       // 'ftyp'
+    if (type == 0x6A703268) {                                  // 'jp2h'
+      if (!ftyp) return (size_t)-1;
+      for (size_t q = body; q < next;) {
+        uint32_t st;
+        size_t sb, sn;
+        if (!box(q, next, st, sb, sn)) return (size_t)-1;
+        if (st == 0x636F6C72 && sn - sb >= 3 && !H.jp2_colr_method) {  // 'colr': the first one counts
+          H.jp2_colr_method = d[sb];
+          if (d[sb] == 1 && sn - sb >= 7) H.jp2_colr_enum = (int)be32(sb + 3);
+        }
+        q = sn;
+      }
+      jp2h = true;
+    }
+    pos = next;
   }
-  return 0;
 }
 
 namespace {
@@ -452,6 +484,11 @@ int finish_coding(StreamHeader &H, const StreamHeader *main) {
     }
   }
   if (main && (H.reversible[0] != main->reversible[0] || H.mct != main->mct)) return PARSE_ERR_UNSUPPORTED;
+  // the inverse RCT / ICT combines the first three components sample by sample, which needs
+  // them sampled alike (T.800 G.1)
+  if (H.mct && H.ncomp >= 3)
+    for (int c = 1; c < 3; ++c)
+      if (H.sub_x[c] != H.sub_x[0] || H.sub_y[c] != H.sub_y[0]) return PARSE_ERR_UNSUPPORTED;
   return PARSE_OK;
 }
 
@@ -459,8 +496,12 @@ int finish_coding(StreamHeader &H, const StreamHeader *main) {
 
 int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   H = StreamHeader();
-  size_t off = find_codestream(data, len);
+  size_t off = find_codestream(data, len, H);
   if (off == (size_t)-1) return PARSE_ERR_MARKER;
+  // an enumerated colour space other than sRGB, greyscale or sYCC is refused, as the
+  // reference refuses it (dec_jp2.cpp:462-464)
+  if (H.jp2_colr_method == 1 && H.jp2_colr_enum != 16 && H.jp2_colr_enum != 17 && H.jp2_colr_enum != 18)
+    return PARSE_ERR_UNSUPPORTED;
   H.cs_offset = off;
   Reader r{data + off, data + len};
   if (r.u16() != 0xFF4F) return PARSE_ERR_MARKER;
@@ -542,7 +583,9 @@ int parse_header(const uint8_t *data, size_t len, StreamHeader &H) {
   // tile indices are 16-bit, 65535 excluded (T.800 A.4.2)
   if ((int64_t)H.ntx() * H.nty() > 65535) return PARSE_ERR_INVALID;
   for (int c = 0; c < H.ncomp; ++c) {
-    if (H.sub_x[c] != 1 || H.sub_y[c] != 1) return PARSE_ERR_UNSUPPORTED;
+    // component separation XRsiz / YRsiz (T.800 A.5.1: 1..255); sub-sampled components are
+    // decoded on their own grids (B.2-B.3) and replicated onto the picture grid on output
+    if (H.sub_x[c] < 1 || H.sub_y[c] < 1) return PARSE_ERR_INVALID;
     if (H.depth[c] > 16 || H.depth[c] != H.depth[0]) return PARSE_ERR_UNSUPPORTED;
     // signed samples take no DC level shift (T.800 G.1.2); the output stages apply the
     // unsigned shift, so such pictures are refused rather than decoded wrongly
@@ -724,8 +767,6 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
   std::vector<TileOut> outs(ntiles);
   P.out_w = H.out_w(discard);
   P.out_h = H.out_h(discard);
-  // tile-components are placed relative to the image origin at the output resolution
-  const int ox = ceil_div_pow2(H.x0, discard), oy = ceil_div_pow2(H.y0, discard);
   auto process_tile = [&](int t, TileOut &out) -> int {
     uint64_t coef_total = 0;
     const StreamHeader &TH = tile_header(t);
@@ -740,10 +781,12 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
     for (int c = 0; c < TH.ncomp; ++c) {
       TCState &TC = tcs[c];
       TC.comp = c;
-      TC.x0 = tx0;
-      TC.y0 = ty0;
-      TC.x1 = tx1;
-      TC.y1 = ty1;
+      // the tile on component c's own grid (T.800 B.3: ceil of the reference-grid bounds
+      // over XRsiz / YRsiz)
+      TC.x0 = ceil_div(tx0, TH.sub_x[c]);
+      TC.y0 = ceil_div(ty0, TH.sub_y[c]);
+      TC.x1 = ceil_div(tx1, TH.sub_x[c]);
+      TC.y1 = ceil_div(ty1, TH.sub_y[c]);
       TC.levels = TH.levels[c];
       const int L = TC.levels;
       TC.res.resize(L + 1);
@@ -1046,10 +1089,13 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
             const int64_t rx0 = (int64_t)R.x0 << lv, ry0 = (int64_t)R.y0 << lv;
             const int64_t spx = (int64_t)1 << (ppx + lv), spy = (int64_t)1 << (ppy + lv);
             const int px0 = R.x0 >> ppx, py0 = R.y0 >> ppy;
+            // reference-grid coordinates: component units times XRsiz / YRsiz; a precinct
+            // starting before the tile is visited at the tile's own corner
+            const int64_t dx = TH.sub_x[c], dy = TH.sub_y[c];
             for (int pj = 0; pj < R.npy; ++pj) {
-              const int64_t y = pj ? (int64_t)(py0 + pj) * spy : ((ry0 % spy) ? TC.y0 : ry0);
+              const int64_t y = pj ? (int64_t)(py0 + pj) * spy * dy : ((ry0 % spy) ? ty0 : ry0 * dy);
               for (int pi = 0; pi < R.npx; ++pi) {
-                const int64_t x = pi ? (int64_t)(px0 + pi) * spx : ((rx0 % spx) ? TC.x0 : rx0);
+                const int64_t x = pi ? (int64_t)(px0 + pi) * spx * dx : ((rx0 % spx) ? tx0 : rx0 * dx);
                 pv.push_back({y, x, r, c, pj * R.npx + pi});
               }
             }
@@ -1091,8 +1137,9 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
       tc.tile = t;
       tc.levels = keep;
       const ResState &Rtop = TC.res[keep];
-      tc.x0 = Rtop.x0 - ox;
-      tc.y0 = Rtop.y0 - oy;
+      // relative to the component's own image origin at the output resolution
+      tc.x0 = Rtop.x0 - ceil_div_pow2(ceil_div(TH.x0, TH.sub_x[c]), discard);
+      tc.y0 = Rtop.y0 - ceil_div_pow2(ceil_div(TH.y0, TH.sub_y[c]), discard);
       tc.w = Rtop.x1 - Rtop.x0;
       tc.h = Rtop.y1 - Rtop.y0;
       for (int r = 0; r <= keep; ++r) {
@@ -1250,6 +1297,17 @@ int build_plan(const uint8_t *data, size_t len, const DecodeOptions &opt, ImageP
   I.num_segs = (int32_t)P.seglens.size();
   I.coded_bytes = P.bytes.size();
   I.coef_elems = coef_total;
+  I.origin_x = ceil_div_pow2(H.x0, discard);
+  I.origin_y = ceil_div_pow2(H.y0, discard);
+  for (int c = 0; c < H.ncomp; ++c) {
+    I.sub_x[c] = H.sub_x[c];
+    I.sub_y[c] = H.sub_y[c];
+    const int cx0 = ceil_div(H.x0, H.sub_x[c]), cy0 = ceil_div(H.y0, H.sub_y[c]);
+    I.comp_x0[c] = ceil_div_pow2(cx0, discard);
+    I.comp_y0[c] = ceil_div_pow2(cy0, discard);
+    I.comp_w[c] = ceil_div_pow2(ceil_div(H.width, H.sub_x[c]), discard) - I.comp_x0[c];
+    I.comp_h[c] = ceil_div_pow2(ceil_div(H.height, H.sub_y[c]), discard) - I.comp_y0[c];
+  }
   return PARSE_OK;
 }
 

@@ -92,11 +92,22 @@ struct StreamHeader {
   std::vector<PocEntry> poc;  /* progression volumes (empty: the COD order over everything) */
   std::vector<uint8_t> ppm;   /* main header only: PPM payloads (Nppm + packed headers per tile-part) */
   bool has_ppm = false;
+  int jp2_colr_method = 0;  /* JP2 colour specification box: method (0 = none / raw codestream) */
+  int jp2_colr_enum = 0;    /* its enumerated colour space (16 sRGB, 17 greyscale, 18 sYCC) */
   size_t header_len = 0;    /* bytes up to the first SOT */
   size_t cs_offset = 0;     /* offset of SOC inside the input (JP2 wrapper) */
   /* picture size: the reference grid from the image origin (x0, y0) to (width, height) */
   int image_w() const { return width - x0; }
   int image_h() const { return height - y0; }
+  /* component c's grid at 1/2^d resolution (T.800 B.2): origin and size */
+  int comp_x0(int c, int d) const { return (int)(((((int64_t)x0 + sub_x[c] - 1) / sub_x[c]) + (1LL << d) - 1) >> d); }
+  int comp_y0(int c, int d) const { return (int)(((((int64_t)y0 + sub_y[c] - 1) / sub_y[c]) + (1LL << d) - 1) >> d); }
+  int comp_w(int c, int d) const {
+    return (int)(((((int64_t)width + sub_x[c] - 1) / sub_x[c]) + (1LL << d) - 1) >> d) - comp_x0(c, d);
+  }
+  int comp_h(int c, int d) const {
+    return (int)(((((int64_t)height + sub_y[c] - 1) / sub_y[c]) + (1LL << d) - 1) >> d) - comp_y0(c, d);
+  }
   /* picture size at 1/2^d resolution (T.800 B.5: ceil(width / 2^d) - ceil(x0 / 2^d)) */
   int out_w(int d) const { return (int)((((int64_t)width + (1LL << d) - 1) >> d) - (((int64_t)x0 + (1LL << d) - 1) >> d)); }
   int out_h(int d) const { return (int)((((int64_t)height + (1LL << d) - 1) >> d) - (((int64_t)y0 + (1LL << d) - 1) >> d)); }

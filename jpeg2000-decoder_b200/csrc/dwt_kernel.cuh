@@ -61,6 +61,14 @@ struct OutGroup {
   int16_t fmt, bitdepth;
   int8_t rev, mct, ncomp, checkout;  // checkout: reference mCheckOutComponent, -1 = all
   int32_t tiles_x;
+  // sub-sampled components (SIZ XRsiz / YRsiz > 1): pixel (x0 + xx, y0 + yy) shows sample
+  // (floor((ax + xx) / sx[c]) - cx[c], floor((ay + yy) / sy[c]) - cy[c]) of component c's
+  // tile-component (clamped to its cw x ch samples), ax / ay being the tile's absolute
+  // pixel origin and cx / cy the tile-component's absolute origin on the component's grid
+  int32_t ax, ay;
+  int32_t cx[4], cy[4], cw[4], ch[4];
+  uint8_t sx[4], sy[4];
+  int8_t sampled;
 };
 struct OutTask {
   uint32_t group;
@@ -440,15 +448,24 @@ __global__ void __launch_bounds__(256) output_kernel(const OutGroup *__restrict_
     for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
       const int yy = oy + i / 64, xx = ox + i % 64;
       if (yy >= G.h || xx >= G.w) continue;
+      size_t at[4];
+      for (int c = 0; c < 4; ++c) {
+        at[c] = (size_t)yy * G.stride[c] + xx;
+        if (G.sampled && have[c]) {  // replicate a sub-sampled component's nearest-left sample
+          const int i = min(max((G.ax + xx) / G.sx[c] - G.cx[c], 0), G.cw[c] - 1);
+          const int j = min(max((G.ay + yy) / G.sy[c] - G.cy[c], 0), G.ch[c] - 1);
+          at[c] = (size_t)j * G.stride[c] + i;
+        }
+      }
       if (G.rev) {
         int32_t v[4] = {0, 0, 0, 0};
         for (int c = 0; c < 4; ++c)
-          if (have[c]) v[c] = ((const int32_t *)cb[c])[(size_t)yy * G.stride[c] + xx];
+          if (have[c]) v[c] = ((const int32_t *)cb[c])[at[c]];
         emit_pixel<int32_t>(G, out, yy, xx, v, have);
       } else {
         float v[4] = {0.f, 0.f, 0.f, 0.f};
         for (int c = 0; c < 4; ++c)
-          if (have[c]) v[c] = ((const float *)cb[c])[(size_t)yy * G.stride[c] + xx];
+          if (have[c]) v[c] = ((const float *)cb[c])[at[c]];
         emit_pixel<float>(G, out, yy, xx, v, have);
       }
     }

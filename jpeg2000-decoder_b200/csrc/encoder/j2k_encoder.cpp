@@ -912,7 +912,19 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
   if (P->num_layers < 1 || P->num_layers > 32) return -5;
   const int TW = P->tile_w > 0 ? P->tile_w : W, TH = P->tile_h > 0 ? P->tile_h : H;
   if (P->tile_w > 0 && ((TW % (1 << L)) || (TH % (1 << L)))) return -7;  // even origins at all levels
+  int dx[4], dy[4];
+  for (int c = 0; c < 4; ++c) {
+    dx[c] = P->sub_x[c] > 1 ? P->sub_x[c] : 1;
+    dy[c] = P->sub_y[c] > 1 ? P->sub_y[c] : 1;
+    if (dx[c] > 255 || dy[c] > 255) return -12;
+    // tile-components start on even coordinates at every level
+    if (c < ncomp && P->tile_w > 0 && ((TW % dx[c]) || (TH % dy[c]) || ((TW / dx[c]) % (1 << L)) ||
+                                       ((TH / dy[c]) % (1 << L))))
+      return -12;
+  }
   const bool rev = P->reversible != 0;
+  const bool same3 = ncomp >= 3 && dx[1] == dx[0] && dx[2] == dx[0] && dy[1] == dy[0] && dy[2] == dy[0];
+  if (P->use_mct && ncomp >= 3 && !same3) return -12;  // the MCT needs equally sampled components
   const bool mct = P->use_mct && ncomp >= 3;
   const int mode =
       P->mode & (J2KENC_BYPASS | J2KENC_RESET | J2KENC_TERMALL | J2KENC_CAUSAL | J2KENC_PTERM | J2KENC_SEGSYM);
@@ -999,19 +1011,27 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
       int t = next_tile.fetch_add(1);
       if (t >= (int)tiles.size()) break;
       Tile &T = tiles[t];
-      int tw = T.x1 - T.x0, th = T.y1 - T.y0;
-      size_t np = (size_t)tw * th;
-      // DC shift + MCT
-      std::vector<std::vector<double>> cd(ncomp, std::vector<double>(np));
-      std::vector<std::vector<int64_t>> ci(ncomp, std::vector<int64_t>(np));
-      for (int c = 0; c < ncomp; ++c)
-        for (int y = 0; y < th; ++y)
-          for (int x = 0; x < tw; ++x) {
-            int64_t v = (int64_t)planes[(size_t)c * W * H + (size_t)(T.y0 + y) * W + T.x0 + x] - (1 << (B - 1));
-            ci[c][(size_t)y * tw + x] = v;
-            cd[c][(size_t)y * tw + x] = (double)v;
+      // DC shift + MCT; component c covers [ceil(x0 / dx), ceil(x1 / dx)) of its own grid
+      // (T.800 B.2-B.3), its sample (i, j) taken from the plane at (i * dx, j * dy)
+      std::vector<std::vector<double>> cd(ncomp);
+      std::vector<std::vector<int64_t>> ci(ncomp);
+      int ctw[4], cth[4];
+      for (int c = 0; c < ncomp; ++c) {
+        const int cx0 = ceil_div(T.x0, dx[c]), cy0 = ceil_div(T.y0, dy[c]);
+        ctw[c] = ceil_div(T.x1, dx[c]) - cx0;
+        cth[c] = ceil_div(T.y1, dy[c]) - cy0;
+        cd[c].resize((size_t)ctw[c] * cth[c]);
+        ci[c].resize((size_t)ctw[c] * cth[c]);
+        for (int y = 0; y < cth[c]; ++y)
+          for (int x = 0; x < ctw[c]; ++x) {
+            const size_t src = (size_t)(cy0 + y) * dy[c] * W + (size_t)(cx0 + x) * dx[c];
+            int64_t v = (int64_t)planes[(size_t)c * W * H + src] - (1 << (B - 1));
+            ci[c][(size_t)y * ctw[c] + x] = v;
+            cd[c][(size_t)y * ctw[c] + x] = (double)v;
           }
+      }
       if (mct) {
+        const size_t np = (size_t)ctw[0] * cth[0];
         for (size_t i = 0; i < np; ++i) {
           if (rev) {
             int64_t r = ci[0][i], g = ci[1][i], b = ci[2][i];
@@ -1030,6 +1050,7 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
       qb[t].resize(ncomp);
       for (int c = 0; c < ncomp; ++c) {
         // in-place Mallat decomposition over the tile-component
+        const int tw = ctw[c], th = cth[c];
         int cw = tw, ch = th;
         std::vector<int64_t> &I = ci[c];
         std::vector<double> &D = cd[c];
@@ -1151,10 +1172,10 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
     T.comps.resize(ncomp);
     for (int c = 0; c < ncomp; ++c) {
       TileComp &TC = T.comps[c];
-      TC.x0 = T.x0;
-      TC.y0 = T.y0;
-      TC.x1 = T.x1;
-      TC.y1 = T.y1;
+      TC.x0 = ceil_div(T.x0, dx[c]);
+      TC.y0 = ceil_div(T.y0, dy[c]);
+      TC.x1 = ceil_div(T.x1, dx[c]);
+      TC.y1 = ceil_div(T.y1, dy[c]);
       TC.res.resize(L + 1);
       for (int r = 0; r <= L; ++r) {
         Resolution &R = TC.res[r];
@@ -1355,8 +1376,8 @@ extern "C" int j2kenc_encode(const uint16_t *planes, int W, int H, int ncomp, in
   put_u16(cs, ncomp);
   for (int c = 0; c < ncomp; ++c) {
     cs.push_back((uint8_t)(B - 1));
-    cs.push_back(1);
-    cs.push_back(1);
+    cs.push_back((uint8_t)dx[c]);
+    cs.push_back((uint8_t)dy[c]);
   }
   // COD
   put_u16(cs, 0xFF52);

@@ -8,7 +8,8 @@
  * quality layers chosen by slope thresholds, LRCP/RLCP/RPCL/PCRL/CPRL progression with one
  * precinct per resolution, progression volumes (POC, main or tile-part header), tile-parts
  * (optionally interleaved across tiles), SOP / EPH markers, packed packet headers (PPM or
- * PPT), and the BYPASS / RESET / TERMALL / CAUSAL / SEGSYM mode switches.
+ * PPT), the BYPASS / RESET / TERMALL / CAUSAL / SEGSYM mode switches, and sub-sampled
+ * components (XRsiz / YRsiz, e.g. YCbCr 4:2:0 and 4:2:2).
  *
  * The irreversible path writes one guard bit by default: the reference's Tier-1 places the
  * most significant magnitude bit at (expn - 1 - missing) (decoder/codec/src/
@@ -61,6 +62,10 @@ typedef struct j2kenc_params {
   int poc[8][6];      /* per volume: first resolution, first component, layer end, resolution end,
                          component end, progression */
   int poc_in_tiles;   /* 0: POC in the main header; 1: in the first tile-part header of each tile */
+  int sub_x[4], sub_y[4]; /* component sub-sampling XRsiz / YRsiz (0 or 1: none).  Component c keeps
+                             the samples of its plane at reference-grid points (i * sub_x, j * sub_y);
+                             the tile size over each factor must be a multiple of 2^levels, and
+                             the MCT needs the first three components sampled alike */
 } j2kenc_params;
 
 void j2kenc_default_params(j2kenc_params *p);

@@ -427,6 +427,8 @@ extern "C" int j2k_gpu_batch_add(j2k_gpu_ctx *c, const j2k_plan *plan, int fmt, 
   if (fmt != J2K_FMT_NONE && j2k_dev::fmt_bytes(fmt) == 0) return J2K_ERR_ARG;
   const j2k_image_info &I = plan->p.info;
   if (I.bitdepth < 1 || I.bitdepth > 16) return J2K_ERR_UNSUPPORTED;
+  // packed pictures are laid on component 0's grid: it must be the picture grid
+  if (fmt != J2K_FMT_NONE && (I.sub_x[0] != 1 || I.sub_y[0] != 1)) return J2K_ERR_UNSUPPORTED;
   BatchImage bi{};
   bi.checkout = -1;
   bi.plan = plan;
@@ -587,7 +589,8 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
           const j2k_tilecomp &tu = p.tilecomps[u];
           if (tu.tile != tc.tile) continue;
           nc++;
-          ok = tu.comp < 3 && tu.levels == tc.levels && tu.w == tc.w && tu.h == tc.h;
+          ok = tu.comp < 3 && tu.levels == tc.levels && tu.w == tc.w && tu.h == tc.h &&
+               p.info.sub_x[tu.comp] == 1 && p.info.sub_y[tu.comp] == 1;
         }
         if (!ok || nc < 1 || nc > 3) continue;
         for (size_t u = 0; u < p.tilecomps.size(); ++u)
@@ -675,6 +678,8 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
         OutGroup G{};
         for (int k = 0; k < 4; ++k) G.comp_buf[k] = -1;
         int nc = 0;
+        G.ax = p.info.origin_x + tc.x0;
+        G.ay = p.info.origin_y + tc.y0;
         for (size_t u = 0; u < p.tilecomps.size(); ++u) {
           const j2k_tilecomp &tu = p.tilecomps[u];
           if (tu.tile != tc.tile || tu.comp >= 4) continue;
@@ -682,6 +687,15 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
           G.comp_buf[tu.comp] = final_buf[u];
           G.stride[tu.comp] = tu.w;
           nc = std::max(nc, tu.comp + 1);
+          // component sampling: the tile-component's absolute origin and size on its grid
+          const int k = tu.comp;
+          G.sx[k] = (uint8_t)p.info.sub_x[k];
+          G.sy[k] = (uint8_t)p.info.sub_y[k];
+          G.cx[k] = p.info.comp_x0[k] + tu.x0;
+          G.cy[k] = p.info.comp_y0[k] + tu.y0;
+          G.cw[k] = tu.w;
+          G.ch[k] = tu.h;
+          if (G.sx[k] != 1 || G.sy[k] != 1) G.sampled = 1;
         }
         G.x0 = tc.x0;
         G.y0 = tc.y0;
@@ -1122,8 +1136,11 @@ extern "C" int j2k_gpu_component_copy(j2k_gpu_ctx *c, int slot, int comp, void *
   if (!c->synced) return J2K_ERR_STATE;
   const BatchImage &im = c->imgs[slot];
   const auto &p = im.plan->p;
-  const size_t need = (size_t)p.info.width * p.info.height * 4;
-  if (bytes < need || comp < 0 || comp >= p.info.ncomp) return J2K_ERR_ARG;
+  if (comp < 0 || comp >= p.info.ncomp) return J2K_ERR_ARG;
+  // the component on its own grid (smaller than the picture when sub-sampled)
+  const int cw = p.info.comp_w[comp], ch = p.info.comp_h[comp];
+  const size_t need = (size_t)cw * ch * 4;
+  if (bytes < need) return J2K_ERR_ARG;
   if (im.fused) return J2K_ERR_STATE;  // last level fused with the output stage
   cudaSetDevice(c->device);
   bool found = false;
@@ -1132,7 +1149,7 @@ extern "C" int j2k_gpu_component_copy(j2k_gpu_ctx *c, int slot, int comp, void *
     found = true;
     const int Lt = tc.levels;
     const void *buf = Lt == 0 ? c->d_A.p : ((Lt & 1) ? c->d_B.p : c->d_C.p);
-    CK(cudaMemcpy2DAsync((uint8_t *)dst + ((size_t)tc.y0 * p.info.width + tc.x0) * 4, (size_t)p.info.width * 4,
+    CK(cudaMemcpy2DAsync((uint8_t *)dst + ((size_t)tc.y0 * cw + tc.x0) * 4, (size_t)cw * 4,
                          (const uint8_t *)buf + (im.coef_base + tc.coef_off) * 4, (size_t)tc.w * 4, (size_t)tc.w * 4,
                          tc.h, cudaMemcpyDeviceToHost, c->user_stream));
   }

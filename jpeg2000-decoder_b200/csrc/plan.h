@@ -55,7 +55,8 @@ typedef struct j2k_cblk {
 /* One tile-component: the inverse DWT/MCT work for one region of the coefficient buffer. */
 typedef struct j2k_tilecomp {
   uint64_t coef_off;   /* element offset of the region */
-  int32_t x0, y0;      /* tile-component origin in the image (reference grid, no subsampling) */
+  int32_t x0, y0;      /* tile-component origin on its component's grid at the output resolution,
+                          relative to the component's origin (j2k_image_info comp_x0 / comp_y0) */
   int32_t w, h;        /* tile-component size */
   int32_t levels;      /* decomposition levels of this tile-component */
   int32_t comp, tile;
@@ -73,6 +74,15 @@ typedef struct j2k_image_info {
   int32_t num_cblks, num_tilecomps, num_segs;
   uint64_t coded_bytes;  /* Tier-1 bytes in the plan */
   uint64_t coef_elems;   /* elements of the coefficient buffer */
+  /* component sampling (SIZ XRsiz / YRsiz) and each component's own grid at the output
+   * resolution: absolute origin and size.  A tile-component's (x0, y0) are relative to its
+   * component's origin.  Picture pixel (X, Y) (relative to the picture origin
+   * origin_x, origin_y) shows component c's sample floor((origin_x + X) / sub_x[c]) -
+   * comp_x0[c] (likewise in y): sub-sampled components are replicated. */
+  int32_t origin_x, origin_y;
+  int32_t sub_x[J2K_MAX_COMPONENTS], sub_y[J2K_MAX_COMPONENTS];
+  int32_t comp_x0[J2K_MAX_COMPONENTS], comp_y0[J2K_MAX_COMPONENTS];
+  int32_t comp_w[J2K_MAX_COMPONENTS], comp_h[J2K_MAX_COMPONENTS];
 } j2k_image_info;
 
 #endif

@@ -50,7 +50,9 @@ class ImageInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int32) for n in (
         "width", "height", "ncomp", "bitdepth", "is_signed", "tile_w", "tile_h", "ntiles_x", "ntiles_y",
         "levels", "reversible", "mct", "layers", "progression", "cbw", "cbh", "cbstyle", "guard_bits",
-        "num_cblks", "num_tilecomps", "num_segs")] + [("coded_bytes", ctypes.c_uint64), ("coef_elems", ctypes.c_uint64)]
+        "num_cblks", "num_tilecomps", "num_segs")] + [("coded_bytes", ctypes.c_uint64), ("coef_elems", ctypes.c_uint64),
+                                                       ("origin_x", ctypes.c_int32), ("origin_y", ctypes.c_int32)] + [
+        (n, ctypes.c_int32 * 4) for n in ("sub_x", "sub_y", "comp_x0", "comp_y0", "comp_w", "comp_h")]
 
 
 class CodeBlock(ctypes.Structure):
@@ -93,7 +95,8 @@ class EncParams(ctypes.Structure):
                 ("mode", ctypes.c_int), ("use_mct", ctypes.c_int), ("guard_bits", ctypes.c_int),
                 ("base_step", ctypes.c_double), ("num_threads", ctypes.c_int), ("markers", ctypes.c_int),
                 ("tile_parts", ctypes.c_int), ("interleave_tile_parts", ctypes.c_int), ("num_poc", ctypes.c_int),
-                ("poc", (ctypes.c_int * 6) * 8), ("poc_in_tiles", ctypes.c_int)]
+                ("poc", (ctypes.c_int * 6) * 8), ("poc_in_tiles", ctypes.c_int),
+                ("sub_x", ctypes.c_int * 4), ("sub_y", ctypes.c_int * 4)]
 
 ENC_SOP, ENC_EPH, ENC_PPM, ENC_PPT = 1, 2, 4, 8
 
@@ -118,6 +121,7 @@ EXPORTS = [
     "j2k_server_release", "j2k_server_drain", "j2k_server_stats_get", "j2k_server_stats_reset",
     "BMI_dec_info", "BMI_dec_init", "BMI_dec_isr", "BMI_dec", "BMI_dec_thumbnail", "BMI_dec_exit",
     "bmi_decoder_init", "bmi_decoder_set_job", "bmi_decoder_decode", "bmi_decoder_predecode",
+    "bmi_decoder_predecode_format",
     "bmi_decoder_status", "bmi_decoder_result", "bmi_decoder_thumbnail", "bmi_decoder_component_int",
     "bmi_decoder_component_float", "bmi_decoder_release", "bmi_decoder_terminate",
 ]
@@ -233,6 +237,10 @@ def encode(planes, bitdepth, **kw):
         if k == "layer_bpp":
             for n, x in enumerate(v):
                 p.layer_bpp[n] = float(x)
+        elif k in ("sub_x", "sub_y"):  # per-component sub-sampling factors
+            arr = getattr(p, k)
+            for n, x in enumerate(v):
+                arr[n] = int(x)
         elif k == "poc":  # list of (RS, CS, LYE, RE, CE, progression)
             p.num_poc = len(v)
             for n, e in enumerate(v):

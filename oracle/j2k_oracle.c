@@ -800,6 +800,15 @@ int oracle_output(const j2k_image_info *info, const j2k_tilecomp *tcs, int ntc, 
             if (!tc3[c]) continue;
             int v;
             size_t oc = (size_t)y * tc3[c]->w + x;
+            if (info->sub_x[c] > 1 || info->sub_y[c] > 1) {
+              /* a sub-sampled component shows its nearest-left sample (replication): the
+               * sample at floor(absolute pixel / XRsiz) of the component's grid */
+              int i = (info->origin_x + t0->x0 + x) / info->sub_x[c] - (info->comp_x0[c] + tc3[c]->x0);
+              int j = (info->origin_y + t0->y0 + y) / info->sub_y[c] - (info->comp_y0[c] + tc3[c]->y0);
+              i = i < 0 ? 0 : (i >= tc3[c]->w ? tc3[c]->w - 1 : i);
+              j = j < 0 ? 0 : (j >= tc3[c]->h ? tc3[c]->h - 1 : j);
+              oc = (size_t)j * tc3[c]->w + i;
+            }
             if (info->reversible) v = ((const int32_t *)coef)[tc3[c]->coef_off + oc];
             else v = (int)((const float *)coef)[tc3[c]->coef_off + oc];
             v += dc;

@@ -440,3 +440,53 @@ def test_bit_depth_extremes_bit_exact(gpu_ctx, depth):
         out, _ = _decode_check(gpu_ctx, cs, native.FMT_48BITS_RGB)
         rgb = out.view(np.uint16).reshape(70, 90, 3)[:, :, ::-1].transpose(2, 0, 1) >> (16 - depth)
         assert np.array_equal(rgb, img), (depth, mode)
+
+
+@pytest.mark.parametrize("kind", ["420", "422", "440"])
+@pytest.mark.parametrize("reversible", [1, 0])
+def test_subsampled_components_bit_exact(gpu_ctx, kind, reversible):
+    """Sub-sampled components (XRsiz / YRsiz): packed output (component planes replicated
+    onto the picture grid) and each component on its own grid equal the oracle; lossless
+    pictures equal their decimated source planes."""
+    from jpeg2000_decoder_b200 import native
+    from test_cpu_subsampling import components_from_coef, subsampled_stream
+    for tiles in (0, 64):
+        cs, img, planes, sx, sy = subsampled_stream(kind, reversible=reversible, tiles=tiles)
+        for fmt in (native.FMT_24BITS_3COMPONENTS, native.FMT_32BITS_4COMPONENTS, native.FMT_24BITS_RGB):
+            out, plan = _decode_check(gpu_ctx, cs, fmt)
+        plan = native.Plan(cs)
+        gpu_ctx.begin()
+        slot = gpu_ctx.add(plan, native.FMT_NONE)
+        gpu_ctx.launch()
+        assert gpu_ctx.sync() == 0
+        _, _, ocoef = oracle_util.oracle_decode(plan, native.FMT_NONE)
+        want = components_from_coef(plan, ocoef)
+        I = plan.info
+        for c in range(3):
+            dt = np.int32 if reversible else np.float32
+            got = np.empty((I.comp_h[c], I.comp_w[c]), dt)
+            rc = native.lib().j2k_gpu_component_copy(gpu_ctx.h, slot, c, got.ctypes.data_as(ctypes.c_void_p), got.nbytes)
+            assert rc == 0
+            ref = want[c].astype(np.int32)  # the oracle's buffer holds int32 (5/3) or float32 bits (9/7)
+            assert np.array_equal(got.view(np.int32), ref), (kind, tiles, c)
+            if reversible:
+                assert np.array_equal(got + 128, planes[c])
+
+
+def test_subsampled_packed_output_needs_full_resolution_first_component(gpu_ctx):
+    """Packed pictures are laid on component 0's grid: a picture whose component 0 is itself
+    sub-sampled is refused for packed output and decodes component by component."""
+    from jpeg2000_decoder_b200 import native, synth
+    img = synth.fields_and_edges(51, 64, 64)[:1]
+    cs = native.encode(img, 8, reversible=1, levels=2, sub_x=[2], sub_y=[2])
+    plan = native.Plan(cs)
+    gpu_ctx.begin()
+    rc = native.lib().j2k_gpu_batch_add(gpu_ctx.h, plan.h, native.FMT_32BITS_4COMPONENTS, 0, None)
+    assert rc == native.J2K_ERR_UNSUPPORTED
+    gpu_ctx.begin()
+    slot = gpu_ctx.add(plan, native.FMT_NONE)
+    gpu_ctx.launch()
+    assert gpu_ctx.sync() == 0
+    got = np.empty((32, 32), np.int32)
+    assert native.lib().j2k_gpu_component_copy(gpu_ctx.h, slot, 0, got.ctypes.data_as(ctypes.c_void_p), got.nbytes) == 0
+    assert np.array_equal(got + 128, img[0][::2, ::2])
