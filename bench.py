@@ -138,6 +138,14 @@ def replica_throughput(units_per_rank, world, steps, total_time_s):
 
 
 # ------------------------------------------------------------------ CPU baselines -------
+def host_cores():
+    """Host threads this process may run on (its CPU affinity), else the machine's count."""
+    try:
+        return len(os.sched_getaffinity(0)) or 1
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
 def reference_sample(name, streams):
     """Codestreams of this workload that the reference's own decoder takes, and what they are.
 
@@ -180,7 +188,7 @@ def reference_cpu(name, streams, fmt, steps, warmup, workers=None, step_seconds=
     cs, what = reference_sample(name, streams)
     if not cs:
         return None
-    workers = workers or os.cpu_count() or 1
+    workers = workers or host_cores()
     fmts = [fmt if fmt is not None else synth.c5_format(c) for c in cs]
 
     def timed(i, n):
@@ -221,7 +229,7 @@ def cpu_decode_sample(streams, fmt, budget_s=15.0, threads=None):
     from jpeg2000_decoder_b200 import build
     build.build_oracle()
     import oracle_util
-    threads = threads or os.cpu_count() or 1
+    threads = threads or host_cores()
     sample = list(streams[:max(1, min(len(streams), threads))])
     used = min(len(sample), threads)
 
