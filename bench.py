@@ -515,7 +515,11 @@ def run_gpu(args, rank, world, dist):
     cfg.update({"parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",
                 "bad_blocks": bad, "cuda_graph": not args.no_graph,
                 "autotuned_t1": ({"form": "compact" if tuned["t1_form"] == 1 else "unrolled",
-                                  "warps_per_cta": tuned["t1_warps_per_cta"]} if tuned else None)})
+                                  "warps_per_cta": tuned["t1_warps_per_cta"]} if tuned else None),
+                "autotuned_dwt": ({"coarse_levels": "one shared-memory kernel" if tuned["dwt_coarse"] == 1
+                                   else "one launch per level",
+                                   "candidates": ["coarse levels (<= 64 a side) in one kernel",
+                                                  "one launch per level"]} if tuned else None)})
     line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(step_ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (9/7) / int32 (5/3)", "data": "synthetic (seeded, project encoder)",
@@ -711,7 +715,7 @@ def run_decode_repeat(args):
     if args.frames > 0:
         streams = streams[:args.frames]
     ctx = native.GpuContext(dev)
-    ctx.set_tuning(t1_form=args.t1_form)
+    ctx.set_tuning(t1_form=args.t1_form, dwt_coarse=args.dwt_coarse)
     plans = [native.Plan(s) for s in streams]
     for it in range(args.decode_repeat):
         ctx.begin()
@@ -747,6 +751,8 @@ def main():
                     help="profiling mode: decode the workload this many times, print stage times, no bench line")
     ap.add_argument("--frames", type=int, default=0, help="profiling mode: only the first N pictures")
     ap.add_argument("--t1-form", type=int, default=0, help="profiling mode: Tier-1 form 0 auto, 1 compact, 2 unrolled")
+    ap.add_argument("--dwt-coarse", type=int, default=0,
+                    help="profiling mode: coarse DWT levels 0 auto, 1 fused into one kernel, 2 one launch per level")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

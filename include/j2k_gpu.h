@@ -151,15 +151,21 @@ typedef struct j2k_gpu_tuning {
   int use_graph;         /* capture Tier-1 + DWT launches of a batch into a CUDA graph */
   int t1_form;           /* Tier-1 kernel form: 0 auto, 1 compact (throughput), 2 unrolled (latency) */
   int t1_latency_waves;  /* auto form: unrolled while code-blocks <= this many x 32 warps x SMs */
+  int dwt_coarse;        /* the coarse levels of each tile-component (resolutions up to 64 samples a
+                            side) in one shared-memory kernel: 0 default (on), 1 on, 2 off (one
+                            launch per level) */
 } j2k_gpu_tuning;
 int j2k_gpu_set_tuning(j2k_gpu_ctx *ctx, const j2k_gpu_tuning *t);
 int j2k_gpu_get_tuning(const j2k_gpu_ctx *ctx, j2k_gpu_tuning *t);
 /* Autotuner: times the staged batch (`iters` runs after one warm-up run per candidate)
  * under each Tier-1 kernel form (compact / unrolled) and CTA width (2, 4, 8 warps) and
  * records the fastest for batches of this many code-blocks (power-of-two bucket); the
- * auto form (t1_form 0) then uses it for every later batch in that bucket.  The context's
- * own tuning is left as it was; `best` / `best_ms` (may be NULL) receive the winner and its
- * Tier-1 time.  The staged batch can be run again afterwards. */
+ * auto form (t1_form 0) then uses it for every later batch in that bucket.  Then, with that
+ * Tier-1 shape, it times the inverse DWT with the coarse levels fused into one
+ * shared-memory kernel and with one launch per level (re-staging the batch for each) and
+ * keeps the faster for dwt_coarse 0.  The context's own tuning is left as it was and the
+ * batch is staged again with it; `best` / `best_ms` (may be NULL) receive the winner and
+ * its Tier-1 time.  The staged batch can be run again afterwards. */
 int j2k_gpu_autotune(j2k_gpu_ctx *ctx, void *stream, int iters, j2k_gpu_tuning *best, float *best_ms);
 
 /* Inverse DWT of one tile-component that allocates no device memory, for callers that

@@ -499,30 +499,48 @@ __global__ void __launch_bounds__(FUSED_THREADS) last_level_output_kernel(const 
     dwt_windows<REV>(S, nc, src, F.rw, F.rh, F.lw, F.lh, F.ll_gain != 0, ll_gain_value, F.refcompat != 0, ox, oy);
     const int ow = min(DWT_T, F.rw - ox), oh = min(DWT_T, F.rh - oy);
     if (G.fmt == 2 && G.bitdepth == 8 && G.mct && nc == 3) {
-      // 24-bit RGB after the inverse MCT (the common path): four pixels per thread, stored
-      // as three 32-bit words when the row allows (bytes B, G, R per pixel)
-      for (int i = threadIdx.x; i < DWT_T * (DWT_T / 4); i += blockDim.x) {
-        const int yy = i / (DWT_T / 4), xx = (i % (DWT_T / 4)) * 4;
+      // 24-bit RGB after the inverse MCT (the common path): sixteen pixels per thread (48
+      // bytes, bytes B, G, R per pixel) go out as three 16-byte stores when the run is
+      // 16-byte aligned and whole, else as 32-bit words or bytes
+      constexpr int RUN = 16;
+      for (int i = threadIdx.x; i < DWT_T * (DWT_T / RUN); i += blockDim.x) {
+        const int yy = i / (DWT_T / RUN), xx = (i % (DWT_T / RUN)) * RUN;
         if (yy >= oh || xx >= ow) continue;
         uint8_t *px = out + G.out_off + ((size_t)(G.y0 + oy + yy) * G.pitch_px + (G.x0 + ox + xx)) * 3;
-        uint32_t bytes[3] = {0, 0, 0};
-        const int npx = min(4, ow - xx);
-        for (int k = 0; k < 4; ++k) {
+        uint32_t words[12];
+#pragma unroll
+        for (int j = 0; j < 12; ++j) words[j] = 0;
+        const int npx = min(RUN, ow - xx);
+#pragma unroll
+        for (int k = 0; k < RUN; ++k) {
           const int o = (yy + DWT_H) * DWT_PITCH + xx + k + DWT_H;
           int rgb[3];
           mct_pixel<T>(S[0].tile[o], S[1].tile[o], S[2].tile[o], 128, 255, rgb);
+#pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int b = k * 3 + j;  // byte j of pixel k: B, G, R
-            bytes[b >> 2] |= (uint32_t)rgb[2 - j] << (8 * (b & 3));
+            words[b >> 2] |= (uint32_t)rgb[2 - j] << (8 * (b & 3));
           }
         }
-        if (npx == 4 && !((uintptr_t)px & 3)) {
-          uint32_t *w = reinterpret_cast<uint32_t *>(px);
-          w[0] = bytes[0];
-          w[1] = bytes[1];
-          w[2] = bytes[2];
+        if (npx == RUN && !((uintptr_t)px & 15)) {
+          uint4 *v = reinterpret_cast<uint4 *>(px);
+          v[0] = make_uint4(words[0], words[1], words[2], words[3]);
+          v[1] = make_uint4(words[4], words[5], words[6], words[7]);
+          v[2] = make_uint4(words[8], words[9], words[10], words[11]);
+        } else if (npx == RUN && !((uintptr_t)px & 3)) {
+#pragma unroll
+          for (int j = 0; j < 12; ++j) reinterpret_cast<uint32_t *>(px)[j] = words[j];
         } else {
-          for (int b = 0; b < npx * 3; ++b) px[b] = (uint8_t)(bytes[b >> 2] >> (8 * (b & 3)));
+          // a partial or unaligned run (picture edge, odd widths): pixel by pixel, recomputed
+          // so that `words` stays in registers
+          for (int k = 0; k < npx; ++k) {
+            const int o = (yy + DWT_H) * DWT_PITCH + xx + k + DWT_H;
+            int rgb[3];
+            mct_pixel<T>(S[0].tile[o], S[1].tile[o], S[2].tile[o], 128, 255, rgb);
+            px[3 * k] = (uint8_t)rgb[2];
+            px[3 * k + 1] = (uint8_t)rgb[1];
+            px[3 * k + 2] = (uint8_t)rgb[0];
+          }
         }
       }
     } else {
@@ -533,6 +551,122 @@ __global__ void __launch_bounds__(FUSED_THREADS) last_level_output_kernel(const 
         for (int c = 0; c < nc; ++c) v[c] = S[c].tile[(yy + DWT_H) * DWT_PITCH + xx + DWT_H];
         emit_pixel<T>(G, out, oy + yy, ox + xx, v, have);
       }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ coarse levels -------
+// The coarsest levels of a tile-component are tiny (a 512x512 tile-component with five
+// levels synthesises 32x32 and 64x64 before its first 128x128 level), so one launch per
+// level leaves the GPU idle between short grids.  Here one CTA synthesises every level up to
+// resolution `rc` of one tile-component in shared memory: the top-left res_w[rc] x res_h[rc]
+// block of the tile-component's Mallat region already holds LL and every band up to that
+// resolution, so it is staged once, each level is rebuilt in place (rows into a second
+// buffer, columns back), and resolution rc is written once to the level buffer the level
+// kernels would have left it in.  Arithmetic is the per-level kernels' (and the oracle's):
+// whole-sample symmetric lifting over the full line, the same rounded float operations,
+// K_lo^2 on a reconstructed 9/7 LL, the reference's 5/3 column end on request.
+constexpr int COARSE_MAX = 64;  // largest resolution edge synthesised here
+struct CoarseTask {
+  uint64_t base;      // element offset of the tile-component region
+  int32_t stride;     // tile-component width
+  int8_t rc;          // resolutions 1..rc are synthesised here
+  int8_t out_dst;     // buffer receiving resolution rc: 1 B, 2 C
+  int8_t refcompat;   // 5/3: reference column-end arithmetic
+  int8_t pad;
+  int16_t res_w[8], res_h[8];  // resolutions 0..rc (rc <= 7: 64 << 7 exceeds any level kept here)
+};
+
+// In-place inverse lifting of one interleaved line of n samples (element stride st), the
+// oracle's line97 / line53: x[-1] = x[1], x[n] = x[n - 2]
+template <bool REV>
+__device__ __forceinline__ void lift_full_line(typename DwtTypes<REV>::T *x, int n, int st) {
+  if (n < 2) return;
+  auto at = [&](int i) -> typename DwtTypes<REV>::T & {
+    const int j = i < 0 ? -i : (i >= n ? 2 * (n - 1) - i : i);
+    return x[j * st];
+  };
+  if constexpr (REV) {
+    for (int i = 0; i < n; i += 2) at(i) = at(i) - ((at(i - 1) + at(i + 1) + 2) >> 2);
+    for (int i = 1; i < n; i += 2) at(i) = at(i) + ((at(i - 1) + at(i + 1)) >> 1);
+  } else {
+    for (int i = 0; i < n; i += 2) at(i) = lift97(at(i), 0.44350685204397f, at(i - 1), at(i + 1));
+    for (int i = 1; i < n; i += 2) at(i) = lift97(at(i), 0.88291107553093f, at(i - 1), at(i + 1));
+    for (int i = 0; i < n; i += 2) at(i) = lift97(at(i), -0.05298011857296f, at(i - 1), at(i + 1));
+    for (int i = 1; i < n; i += 2) at(i) = lift97(at(i), -1.58613434205992f, at(i - 1), at(i + 1));
+  }
+}
+
+template <bool REV>
+__global__ void __launch_bounds__(128) dwt_coarse_kernel(const CoarseTask *__restrict__ tasks, int ntasks, void *bufA,
+                                                          void *bufB, void *bufC, float ll_gain_value) {
+  typedef typename DwtTypes<REV>::T T;
+  constexpr int P = COARSE_MAX + 1;  // odd pitch
+  __shared__ T X[COARSE_MAX * P], Y[COARSE_MAX * P];
+  for (int task = blockIdx.x; task < ntasks; task += gridDim.x) {
+    const CoarseTask tk = tasks[task];
+    const T *A = dwt_buf<REV>(0, bufA, bufB, bufC) + tk.base;
+    T *out = dwt_buf<REV>(tk.out_dst, bufA, bufB, bufC) + tk.base;
+    const int W = tk.res_w[tk.rc], H = tk.res_h[tk.rc];
+    for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
+      const int y = i / W, x = i - y * W;
+      X[y * P + x] = A[(size_t)y * tk.stride + x];
+    }
+    __syncthreads();
+    for (int r = 1; r <= tk.rc; ++r) {
+      const int rw = tk.res_w[r], rh = tk.res_h[r], lw = tk.res_w[r - 1], lh = tk.res_h[r - 1];
+      if (!REV && r > 1) {  // the reconstructed LL entering a finer 9/7 level
+        for (int i = threadIdx.x; i < lw * lh; i += blockDim.x) {
+          const int y = i / lw, x = i - y * lw;
+          X[y * P + x] = (T)__fmul_rn((float)X[y * P + x], ll_gain_value);
+        }
+        __syncthreads();
+      }
+      // rows: interleave low / high parts into Y, lift
+      for (int y = threadIdx.x; y < rh; y += blockDim.x) {
+        T *row = Y + y * P;
+        for (int i = 0; i < rw; ++i) row[i] = X[y * P + ((i & 1) ? lw + (i >> 1) : (i >> 1))];
+        lift_full_line<REV>(row, rw, 1);
+      }
+      __syncthreads();
+      // columns: interleave low / high rows back into X, lift (5/3: the reference's column
+      // end on request, from the column's de-interleaved inputs as in the level kernels)
+      for (int x = threadIdx.x; x < rw; x += blockDim.x) {
+        T *col = X + x;
+        for (int i = 0; i < rh; ++i) col[i * P] = Y[((i & 1) ? lh + (i >> 1) : (i >> 1)) * P + x];
+        if constexpr (REV) {
+          const int n = rh;
+          const bool fix = tk.refcompat && n >= 3;
+          T a = 0, b = 0;
+          if (fix) {
+            if (!(n & 1)) {
+              a = Y[(lh + n / 2 - 2) * P + x];  // H[m - 2]
+            } else {
+              const int m = (n + 1) / 2;
+              b = Y[(lh + (m >= 3 ? m - 3 : 0)) * P + x];  // H[m - 3] (H[0] when m == 2)
+              a = Y[(m - 2) * P + x];                       // L[m - 2]
+            }
+          }
+          lift_full_line<REV>(col, rh, P);
+          if (fix) {
+            if (!(n & 1)) {
+              col[(n - 1) * P] = a + col[(n - 2) * P];
+            } else {
+              const T x1 = a - ((b + 1) >> 1);
+              col[(n - 1) * P] = x1;
+              col[(n - 2) * P] = b + ((x1 + col[(n - 3) * P]) >> 1);
+            }
+          }
+        } else {
+          lift_full_line<REV>(col, rh, P);
+        }
+      }
+      __syncthreads();
+    }
+    for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
+      const int y = i / W, x = i - y * W;
+      out[(size_t)y * tk.stride + x] = X[y * P + x];
     }
     __syncthreads();
   }

@@ -253,6 +253,7 @@ struct j2k_gpu_ctx {
     size_t nq[NQ] = {0}, n_cblks = 0, n_otasks = 0;
     size_t o_cbs = 0, o_ord = 0, o_seg = 0, o_lev = 0, o_dtk = 0, o_grp = 0, o_otk = 0, o_fgr = 0, o_ftk = 0;
     size_t n_ftasks[2] = {0, 0};
+    size_t o_ctk = 0, n_ctasks[2] = {0, 0};  // coarse-level tasks: [0] 9/7, [1] 5/3
     int fwin = 1;
     int maxL = 0;
     std::vector<uint32_t> dtask_off;
@@ -260,7 +261,7 @@ struct j2k_gpu_ctx {
   cudaEvent_t ev[6] = {};  // h2d start, h2d end, Tier-1 end, DWT end, decode end, output copies end
   float t_t1 = 0, t_dwt = 0, t_h2d = 0, t_total = 0;
   int launches = 0;
-  j2k_gpu_tuning tuning{8, 64, 0, 0, 2};
+  j2k_gpu_tuning tuning{8, 64, 0, 0, 2, 0};
   cudaGraphExec_t gexec = nullptr;  // captured decode of the staged batch (tuning.use_graph)
   int graph_launches = 0;
   // autotuned Tier-1 shape per queue-length bucket (floor(log2(code-blocks))): kernel form
@@ -270,6 +271,7 @@ struct j2k_gpu_ctx {
     float t1_ms = 0;
   };
   std::map<int, TuneEntry> tune_table;
+  int dwt_auto = 0;  // autotuned coarse-level choice (1 on, 2 off) for dwt_coarse 0; 0 = not tuned (on)
   int sm_count = 148;
   size_t smem_optin = 227 * 1024;
 };
@@ -401,7 +403,8 @@ extern "C" int j2k_gpu_set_tuning(j2k_gpu_ctx *c, const j2k_gpu_tuning *t) {
   if (n.dwt_tile != 64) return J2K_ERR_UNSUPPORTED;  // the level kernels are built for 64x64 tiles
   if (n.t1_form < 0 || n.t1_form > 2) n.t1_form = 0;
   if (n.t1_latency_waves <= 0) n.t1_latency_waves = 2;
-  if (n.use_graph != c->tuning.use_graph || n.t1_form != c->tuning.t1_form ||
+  if (n.dwt_coarse < 0 || n.dwt_coarse > 2) n.dwt_coarse = 0;  // takes effect at the next batch_stage
+  if (n.use_graph != c->tuning.use_graph || n.t1_form != c->tuning.t1_form || n.dwt_coarse != c->tuning.dwt_coarse ||
       n.t1_warps_per_cta != c->tuning.t1_warps_per_cta || n.t1_latency_waves != c->tuning.t1_latency_waves)
     drop_graph(c);
   c->tuning = n;
@@ -551,6 +554,8 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::vector<OutTask> otasks;
   std::vector<FusedGroup> fgroups;
   std::vector<OutTask> ftasks[2];  // fused last levels: [0] 9/7, [1] 5/3
+  std::vector<CoarseTask> ctasks[2];  // coarse levels synthesised in shared memory: [0] 9/7, [1] 5/3
+  const bool coarse_on = c->tuning.dwt_coarse == 1 || (c->tuning.dwt_coarse == 0 && c->dwt_auto != 2);
   int fwin = 1;
   uint64_t byte_base = 0;
   uint32_t seg_base = 0;
@@ -598,13 +603,33 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
         im.fused = true;
       }
     }
-    // DWT levels of every tile-component, aligned so that all finish at the last step
+    // DWT levels of every tile-component, aligned so that all finish at the last step; the
+    // coarse levels (every resolution up to COARSE_MAX samples a side, below a fused last
+    // level) go to one shared-memory kernel instead
     std::vector<int8_t> final_buf(p.tilecomps.size());
     for (size_t t = 0; t < p.tilecomps.size(); ++t) {
       const j2k_tilecomp &tc = p.tilecomps[t];
       const int Lt = tc.levels;
       final_buf[t] = Lt == 0 ? 0 : ((Lt & 1) ? 1 : 2);
-      for (int r = 1; r <= Lt; ++r) {
+      int rc = 0;
+      if (coarse_on) {
+        const int top = std::min(fuse[t] ? Lt - 1 : Lt, 7);
+        while (rc < top && tc.res_w[rc + 1] <= COARSE_MAX && tc.res_h[rc + 1] <= COARSE_MAX) ++rc;
+        if (rc >= 1) {
+          CoarseTask ck{};
+          ck.base = im.coef_base + tc.coef_off;
+          ck.stride = tc.w;
+          ck.rc = (int8_t)rc;
+          ck.out_dst = (int8_t)((rc & 1) ? 1 : 2);
+          ck.refcompat = (int8_t)refc;
+          for (int r = 0; r <= rc; ++r) {
+            ck.res_w[r] = (int16_t)tc.res_w[r];
+            ck.res_h[r] = (int16_t)tc.res_h[r];
+          }
+          ctasks[rev ? 1 : 0].push_back(ck);
+        }
+      }
+      for (int r = rc + 1; r <= Lt; ++r) {
         DwtLevel L{};
         L.base = im.coef_base + tc.coef_off;
         L.stride = tc.w;
@@ -750,7 +775,8 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   size_t o_otk = align_up(o_grp + groups.size() * sizeof(OutGroup), 256);
   size_t o_fgr = align_up(o_otk + otasks.size() * sizeof(OutTask), 256);
   size_t o_ftk = align_up(o_fgr + fgroups.size() * sizeof(FusedGroup), 256);
-  size_t o_byt = align_up(o_ftk + (ftasks[0].size() + ftasks[1].size()) * sizeof(OutTask), 256);
+  size_t o_ctk = align_up(o_ftk + (ftasks[0].size() + ftasks[1].size()) * sizeof(OutTask), 256);
+  size_t o_byt = align_up(o_ctk + (ctasks[0].size() + ctasks[1].size()) * sizeof(CoarseTask), 256);
   size_t total = align_up(o_byt + S.bytes + 16, 256);
   if (c->h_stage_cap < total) {
     // grow by half again at least: page-locking is slow and freeing it synchronises
@@ -781,6 +807,8 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::memcpy(H + o_fgr, fgroups.data(), fgroups.size() * sizeof(FusedGroup));
   std::memcpy(H + o_ftk, ftasks[0].data(), ftasks[0].size() * sizeof(OutTask));
   std::memcpy(H + o_ftk + ftasks[0].size() * sizeof(OutTask), ftasks[1].data(), ftasks[1].size() * sizeof(OutTask));
+  std::memcpy(H + o_ctk, ctasks[0].data(), ctasks[0].size() * sizeof(CoarseTask));
+  std::memcpy(H + o_ctk + ctasks[0].size() * sizeof(CoarseTask), ctasks[1].data(), ctasks[1].size() * sizeof(CoarseTask));
   {
     // coded bytes of every image, copied by a few threads when there are many
     std::vector<std::pair<size_t, const j2k::ByteBuffer *>> parts;
@@ -828,6 +856,9 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   c->sg.o_ftk = o_ftk;
   c->sg.n_ftasks[0] = ftasks[0].size();
   c->sg.n_ftasks[1] = ftasks[1].size();
+  c->sg.o_ctk = o_ctk;
+  c->sg.n_ctasks[0] = ctasks[0].size();
+  c->sg.n_ctasks[1] = ctasks[1].size();
   c->sg.fwin = fwin;
   c->sg.o_cbs = o_cbs;
   c->sg.o_ord = o_ord;
@@ -903,6 +934,14 @@ int enqueue_decode(j2k_gpu_ctx *c, cudaStream_t st, bool capturing) {
   const DwtTask *d_dtk = (const DwtTask *)(D + o_dtk);
   const float llg = j2k::irrev_ll_gain();
   const int dwt_cap = c->sm_count * 32;  // grid-stride cap: about three waves of resident CTAs
+  for (int k = 0; k < 2; ++k) {
+    const int n = (int)G.n_ctasks[k];
+    if (!n) continue;
+    const CoarseTask *ct = (const CoarseTask *)(D + G.o_ctk) + (k ? G.n_ctasks[0] : 0);
+    if (k) dwt_coarse_kernel<true><<<std::min(n, dwt_cap), 128, 0, st>>>(ct, n, c->d_A.p, c->d_B.p, c->d_C.p, llg);
+    else dwt_coarse_kernel<false><<<std::min(n, dwt_cap), 128, 0, st>>>(ct, n, c->d_A.p, c->d_B.p, c->d_C.p, llg);
+    c->launches++;
+  }
   for (int s = 0; s < maxL; ++s) {
     int n_rev = (int)(dtask_off[2 * s + 1] - dtask_off[2 * s]);
     int n_irr = (int)(dtask_off[2 * s + 2] - dtask_off[2 * s + 1]);
@@ -1200,12 +1239,44 @@ extern "C" int j2k_gpu_autotune(j2k_gpu_ctx *c, void *stream, int iters, j2k_gpu
       }
     }
   c->tune_table[bucket] = win;
+  // DWT: the coarse levels in one shared-memory kernel, or one launch per level.  The choice
+  // shapes the staged task tables, so each candidate re-stages the batch; the winner is kept
+  // for the auto setting (dwt_coarse 0) and the batch is staged again with the caller's
+  // tuning at the end.
+  int dwt_win = 1;
+  float dwt_best = 1e30f;
+  for (int cand : {1, 2}) {
+    j2k_gpu_tuning t = saved;
+    t.t1_form = win.form;
+    t.t1_warps_per_cta = win.warps;
+    t.use_graph = 0;
+    t.dwt_coarse = cand;
+    int rc = j2k_gpu_set_tuning(c, &t);
+    if (rc == J2K_OK) rc = j2k_gpu_batch_stage(c, stream);
+    float tmin = 1e30f;
+    for (int i = 0; rc == J2K_OK && i <= iters; ++i) {
+      if ((rc = j2k_gpu_batch_run(c, stream)) != J2K_OK || (rc = j2k_gpu_batch_sync(c, -1)) != J2K_OK) break;
+      if (i > 0) tmin = std::min(tmin, c->t_dwt);
+    }
+    if (rc != J2K_OK) {
+      c->tuning = saved;
+      return rc;
+    }
+    if (tmin < dwt_best) {
+      dwt_best = tmin;
+      dwt_win = cand;
+    }
+  }
+  c->dwt_auto = dwt_win;
   c->tuning = saved;
+  const int rs = j2k_gpu_batch_stage(c, stream);
+  if (rs != J2K_OK) return rs;
   drop_graph(c);
   if (best) {
     *best = saved;
     best->t1_form = win.form;
     best->t1_warps_per_cta = win.warps;
+    best->dwt_coarse = dwt_win;
   }
   if (best_ms) *best_ms = win.t1_ms;
   return J2K_OK;

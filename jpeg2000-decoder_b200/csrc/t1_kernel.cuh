@@ -469,9 +469,14 @@ __device__ __forceinline__ uint32_t cleanup_column(const BlockSmem &b, uint32_t 
 // (C >= k*Qe and A - k*Qe >= 0x8000, scaled) is consumed in one step: A -= k*Qe, C -= k*Qe.
 // Each pass inlines its decision sites once, without unrolling over the four rows, so the
 // kernel stays small enough for the instruction cache when many warps are resident.
-template <bool UNROLLED>
-__device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p, int pass, bool israw,
-                                         const uint8_t *zc, Mq &mq, Raw &raw, const T1Tables &T, int lane) {
+// PASS (P_SIGPROP / P_MAGREF / P_CLEANUP) and RAW (a bypass segment: raw bits instead of MQ
+// symbols) are compile-time constants, so each instantiation carries only its own pass's
+// column code and no decision tests either flag at run time.
+template <bool UNROLLED, int PASS, bool RAW>
+__device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p, const uint8_t *zc, Mq &mq, Raw &raw,
+                                         const T1Tables &T, int lane) {
+  constexpr int pass = PASS;
+  constexpr bool israw = RAW;
   for (int s = 0; s < stripes; ++s) {
     uint32_t *row = cword(b, s, 0);
     uint8_t *rrow = b.rf + s * b.gap;
@@ -691,7 +696,11 @@ __device__ __forceinline__ int decode_block(const j2k_cblk &cb, const uint8_t *_
       else mq_init(mq, data + seg_pos, len);
       seg_pos += len;
     }
-    run_pass<UNROLLED>(b, stripes, bit_plane, type, israw, zc, mq, raw, T, lane);
+    if (type == P_CLEANUP) run_pass<UNROLLED, P_CLEANUP, false>(b, stripes, bit_plane, zc, mq, raw, T, lane);
+    else if (type == P_SIGPROP && israw) run_pass<UNROLLED, P_SIGPROP, true>(b, stripes, bit_plane, zc, mq, raw, T, lane);
+    else if (type == P_SIGPROP) run_pass<UNROLLED, P_SIGPROP, false>(b, stripes, bit_plane, zc, mq, raw, T, lane);
+    else if (israw) run_pass<UNROLLED, P_MAGREF, true>(b, stripes, bit_plane, zc, mq, raw, T, lane);
+    else run_pass<UNROLLED, P_MAGREF, false>(b, stripes, bit_plane, zc, mq, raw, T, lane);
     if (type == 2 && (cb.flags & J2K_CB_SEGSYM))
       for (int i = 0; i < 4; ++i) mq_uniform(mq);
     if (cb.flags & J2K_CB_RESET) {

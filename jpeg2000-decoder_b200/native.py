@@ -72,7 +72,7 @@ class TileComp(ctypes.Structure):
 
 class Tuning(ctypes.Structure):
     _fields_ = [("t1_warps_per_cta", ctypes.c_int), ("dwt_tile", ctypes.c_int), ("use_graph", ctypes.c_int),
-                ("t1_form", ctypes.c_int), ("t1_latency_waves", ctypes.c_int)]
+                ("t1_form", ctypes.c_int), ("t1_latency_waves", ctypes.c_int), ("dwt_coarse", ctypes.c_int)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -410,8 +410,8 @@ class GpuContext:
         self._ck(lib().j2k_gpu_last_launches(self.h, ctypes.byref(n)), "last_launches")
         return n.value
 
-    def set_tuning(self, t1_warps_per_cta=0, dwt_tile=0, use_graph=0, t1_form=0, t1_latency_waves=0):
-        t = Tuning(t1_warps_per_cta, dwt_tile, use_graph, t1_form, t1_latency_waves)
+    def set_tuning(self, t1_warps_per_cta=0, dwt_tile=0, use_graph=0, t1_form=0, t1_latency_waves=0, dwt_coarse=0):
+        t = Tuning(t1_warps_per_cta, dwt_tile, use_graph, t1_form, t1_latency_waves, dwt_coarse)
         self._ck(lib().j2k_gpu_set_tuning(self.h, ctypes.byref(t)), "set_tuning")
 
     def get_tuning(self):
