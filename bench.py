@@ -297,7 +297,7 @@ def run_reference_arm(args, rank, world):
 
 
 # ------------------------------------------------------------------ GPU arm -----------
-def fp64_check(ctx, plans, fmt, frames=2):
+def fp64_check(ctx, plans, fmt, frames=2, fmts=None):
     """PSNR and max-abs of the device's packed 9/7 pictures against an FP64 T.800
     synthesis (tests/fp64_97.py) of the device's own Tier-1 values, on the first `frames`
     pictures of the batch.  Each block's Tier-1 values are its stage-0 coefficients divided
@@ -306,7 +306,9 @@ def fp64_check(ctx, plans, fmt, frames=2):
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import fp64_97
     worst_psnr, worst_abs = float("inf"), 0.0
-    for p in plans[:frames]:
+    for n, p in enumerate(plans[:frames]):
+        if fmts is not None:
+            fmt = fmts[n]
         ctx.begin()
         slot = ctx.add(p, fmt)  # the benched path: last level fused with the ICT and pack
         ctx.launch()
@@ -461,7 +463,7 @@ def run_gpu(args, rank, world, dist):
     # ---- a shortened serving stream (C5 mix) through the continuous-batching service
     serving = None
     if args.workload != "c5" and not args.no_serving:
-        _, spool, _ = workload("c5", True)
+        _, spool, _ = workload("c5", False)  # the full pool of 48 distinct seeded requests
         m = serve_measure(dev, spool, args.serving_requests, args.depth, args.batch_mpix, 0.0, 1, 5 + rank, dist)
         _, serving = serving_summary(m, world)
         serving["stream"] = "C5 mix: %d requests drawn from %d distinct seeded requests" % (
@@ -680,13 +682,24 @@ def run_serve(args, rank, world, dist):
     if rank != 0:
         return
     value, serving = serving_summary(m, world)
+    # FP64 error of the pool's 9/7 requests: the four of them with the fewest pixels that
+    # cover both bit depths
+    irr = sorted((native.Plan(cs) for cs in pool if not native.Plan(cs).info.reversible),
+                 key=lambda p: p.info.width * p.info.height)
+    pick = [p for p in irr if p.info.bitdepth == 8][:2] + [p for p in irr if p.info.bitdepth > 8][:2]
+    fctx = native.GpuContext(dev)
+    fp64 = fp64_check(fctx, pick, None, frames=len(pick),
+                      fmts=[native.FMT_24BITS_RGB if p.info.bitdepth <= 8 else native.FMT_48BITS_RGB for p in pick])
+    fctx.close()
+    if fp64:
+        fp64["requests"] = ["%dx%d %d-bit" % (p.info.width, p.info.height, p.info.bitdepth) for p in pick]
     base = cpu_baseline("c5", pool, None, port_budget=args.cpu_budget)
     order, fmts = m["order"], m["fmts"]
     h2d = sum(len(pool[i]) for i in order)
     cfg = dict(cfg)
     cfg.update({"requests": n_req, "pipeline_depth": args.depth, "batch_mpix_cap": args.batch_mpix,
                 "parallelism": "replicas x%d" % world, "bad_requests": m["bad"],
-                "l2": "inputs differ per request; no flush"})
+                "l2": "inputs differ per request; no flush", "fp64_check": fp64})
     line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpixel/s", "n_gpus": world, "steps": 1,
             "warmup": args.warmup, "ms_per_step": round(m["sat_s"] * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (9/7) / int32 (5/3)",
@@ -745,7 +758,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="skip the Tier-1 shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="enqueue launches instead of replaying a CUDA graph")
     ap.add_argument("--no-serving", action="store_true", help="skip the shortened serving stream of the default line")
-    ap.add_argument("--serving-requests", type=int, default=240, help="requests of the shortened serving stream")
+    ap.add_argument("--serving-requests", type=int, default=480, help="requests of the shortened serving stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error check")
     ap.add_argument("--decode-repeat", type=int, default=0,
                     help="profiling mode: decode the workload this many times, print stage times, no bench line")

@@ -102,7 +102,8 @@ __device__ __forceinline__ void t1_body(const j2k_cblk *__restrict__ cbs, const 
       st = decode_block<UNROLLED>(cb, bytes, seglens, b, T, lane, bit_plane, num_passes);
     }
     // rewrite the block in place: raw sign-magnitude -> dequantised float (9/7) or shifted
-    // integer (5/3); lane 0's atomic updates are made visible first
+    // integer (5/3); the lanes' sample writes are made visible first.  A sample whose
+    // significance bit (context word, shared memory) is clear was never written: it is 0.
     const int w = cb.w, h = cb.h;
     if (st != 9) {
       __threadfence();
@@ -110,8 +111,10 @@ __device__ __forceinline__ void t1_body(const j2k_cblk *__restrict__ cbs, const 
       const bool irrev = (cb.flags & J2K_CB_IRREV) != 0;
       for (int y = 0; y < h; ++y) {
         int32_t *r = blk + (size_t)y * cb.out_stride;
+        const uint32_t sig = ROW_SIG(y & 3);
+        const uint32_t *wrow = cword(b, y >> 2, 0);
         for (int x = lane; x < w; x += 32) {
-          const int32_t v = __ldcg(r + x);
+          const int32_t v = (wrow[x] & sig) ? __ldcg(r + x) : 0;
           if (irrev) *reinterpret_cast<float *>(r + x) = __fmul_rn((float)signmag_to_int(v), cb.gain);
           else r[x] = place53(v, cb.mb);
         }

@@ -29,8 +29,10 @@
  *     consumed in one step: A -= k*Qe, C -= k*Qe;
  *   - samples live in the block's own region of the output buffer, not in shared memory:
  *     they are only written while decoding (significance sets sign + 1.5 * 2^p, a
- *     refinement flips bit p and sets the new midpoint bit), so a stripe column's updates
- *     go out at its end as fire-and-forget atomic XORs from lanes 0..3 in one instruction,
+ *     refinement flips bit p and sets the new midpoint bit), so updates go out as
+ *     fire-and-forget atomic XORs: in the compact form a stripe column's at its end from
+ *     lanes 0..3 in one instruction, in the unrolled form each 32-column chunk's at its end
+ *     from the lanes owning the columns (off the serial chain: C2 Tier-1 10.8 -> 7.9 ms),
  *     and the "first refinement?" context test of the reference ((|v| >> p) < 4, true
  *     exactly on a sample's first refinement) reads a per-sample "refined" bit kept in
  *     shared memory.  A 64x64 block then needs 6 KB of shared memory instead of 13-21 KB,
@@ -237,29 +239,45 @@ __device__ __forceinline__ int raw_bit(Raw &r) {
   return (int)((r.c >> r.ct) & 1);
 }
 
-// ---- samples: raw int32 (bit 31 sign, magnitude with midpoint bit) accumulated in global
-// memory by XOR updates; the block region is zeroed before decoding.  The updates of one
-// stripe column are collected while it is decoded and issued together at its end, one
-// fire-and-forget atomic per row from lanes 0..3 in a single warp instruction (nothing reads
+// ---- samples: raw int32 (bit 31 sign, magnitude with midpoint bit) built in global memory:
+// a sample's significance writes its first value (nothing touched it before), refinements
+// XOR into it; samples that never become significant are never written while decoding (the
+// final rewrite gives them 0 from the significance bits in shared memory), so the block
+// region needs no zero-fill.  The lane that writes a sample's first value also issues its
+// refinements, so each sample's updates stay in program order.  While a 32-column chunk
+// of a stripe is decoded, each column's update goes to the lane that owns the column (one
+// select in the serial loop); at the end of the chunk every lane issues its column's row
+// updates as fire-and-forget atomics, consecutive lanes on consecutive columns (nothing reads
 // the samples while decoding, and XOR updates commute).
 struct Samples {
   int32_t *base;      // the block's first sample in the output buffer
   uint32_t stride;    // elements per row
   int lane;
-  // column update: bits 0..3 rows updated, bits 4..7 the sign (significance) or the
-  // decoded refinement bit of each row
-  __device__ __forceinline__ void apply_sig(int row0, int col, uint32_t upd, int plane) const {
+  // column update `upd`: bits 0..3 rows updated, bits 4..7 the sign (significance pass) or
+  // the decoded refinement bit (refinement pass) of each row
+  // one column's update from lanes 0..3 in one warp instruction, straight from the serial
+  // loop (compact form: cheapest when every resident warp competes for issue slots)
+  template <bool REFINE>
+  __device__ __forceinline__ void apply(int row0, int col, uint32_t upd, int plane) const {
     if (lane < 4 && ((upd >> lane) & 1)) {
-      const uint32_t sign = (upd >> (4 + lane)) & 1;
-      atomicXor(reinterpret_cast<unsigned int *>(base + (size_t)(row0 + lane) * stride + col),
-                (sign << 31) + (1u << plane) + ((1u << plane) >> 1));
+      const uint32_t bit = (upd >> (4 + lane)) & 1;
+      unsigned int *at = reinterpret_cast<unsigned int *>(base + (size_t)(row0 + lane) * stride + col);
+      if (REFINE) atomicXor(at, ((1u - bit) << plane) | ((1u << plane) >> 1));
+      else *at = (bit << 31) + (1u << plane) + ((1u << plane) >> 1);  // first value of the sample
     }
   }
-  __device__ __forceinline__ void apply_ref(int row0, int col, uint32_t upd, int plane) const {
-    if (lane < 4 && ((upd >> lane) & 1)) {
-      const uint32_t sym = (upd >> (4 + lane)) & 1;
-      atomicXor(reinterpret_cast<unsigned int *>(base + (size_t)(row0 + lane) * stride + col),
-                ((1u - sym) << plane) | ((1u << plane) >> 1));
+  // a chunk's updates, each lane issuing its own column's (unrolled form: the serial loop of
+  // a latency-bound batch keeps only a select per column)
+  template <bool REFINE>
+  __device__ __forceinline__ void flush(int row0, int col, uint32_t upd, int plane) const {
+    if (!(upd & 0xF)) return;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!((upd >> k) & 1)) continue;
+      const uint32_t bit = (upd >> (4 + k)) & 1;
+      unsigned int *at = reinterpret_cast<unsigned int *>(base + (size_t)(row0 + k) * stride + col);
+      if (REFINE) atomicXor(at, ((1u - bit) << plane) | ((1u << plane) >> 1));
+      else *at = (bit << 31) + (1u << plane) + ((1u << plane) >> 1);  // first value of the sample
     }
   }
 };
@@ -508,6 +526,7 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
       uint32_t live = __ballot_sync(0xffffffffu, valid && work);
       uint32_t zero = __ballot_sync(0xffffffffu, valid && word == 0);
       uint32_t dirty = 0;
+      uint32_t my_upd = 0;  // this lane's column update, flushed at the end of the chunk
       // compact form: the lanes' cleanup / refinement masks go through shared memory (they
       // depend on a column's own rows only, so they hold while the chunk is decoded; a
       // register copy would raise the register count above the occupancy budget)
@@ -548,7 +567,8 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
         if (pass == P_MAGREF) {
           const uint32_t rows = LP ? lane_mask : lane_masks[bit];
           const uint32_t upd = magref_column<UNROLLED>(b, cw, rows, rrow + col, israw, raw, mq, T);
-          b.sp.apply_ref(4 * s, col, upd, p);
+          if constexpr (UNROLLED) my_upd = lane == bit ? upd : my_upd;
+          else b.sp.apply<true>(4 * s, col, upd, p);
           continue;
         }
         uint32_t upd;
@@ -564,13 +584,15 @@ __device__ __forceinline__ void run_pass(const BlockSmem &b, int stripes, int p,
         }
         *wp = cw;
         const bool newsig = (upd & 0xF) != 0;
-        if (newsig) b.sp.apply_sig(4 * s, col, upd, p);
+        if constexpr (UNROLLED) my_upd = lane == bit ? upd : my_upd;
+        else if (newsig) b.sp.apply<false>(4 * s, col, upd, p);
         if (newsig && bit < 31) {
           if (pass == P_SIGPROP) live |= 1u << (bit + 1);
           zero &= ~(1u << (bit + 1));
           if (LP) dirty |= 1u << (bit + 1);
         }
       }
+      if constexpr (UNROLLED) b.sp.flush<pass == P_MAGREF>(4 * s, c, my_upd, p);
       if (pass == P_CLEANUP) {
         // end of the bit-plane for this chunk's columns: mu |= sigma, pi cleared
         // (bmi_block_decoder.cpp:571-573); no later decision of this pass reads a column's
@@ -624,14 +646,11 @@ __device__ __forceinline__ int decode_block(const j2k_cblk &cb, const uint8_t *_
                             const BlockSmem &b, const T1Tables &T, int lane, int bit_plane, int num_passes) {
   const int w = cb.w, h = cb.h;
   const int stripes = (h + 3) >> 2;
-  // clear the block's samples (output region), context words and refinement bits; mark
-  // OOB columns and a partial last stripe
-  for (int y = 0; y < h; ++y)
-    for (int x = lane; x < w; x += 32) b.sp.base[(size_t)y * b.sp.stride + x] = 0;
+  // clear the context words and refinement bits (the samples need no clearing: see
+  // Samples); mark OOB columns and a partial last stripe
   const int nwords = (stripes + 2) * b.gap + 2;
   for (int i = lane; i < nwords; i += 32) b.cw[i] = 0;
   for (int i = lane; i < stripes * b.gap; i += 32) b.rf[i] = 0;
-  __threadfence();  // the zeros reach L2 before lane 0's atomic updates
   __syncwarp();
   const uint32_t oob = CHI_ALL;
   for (int s = lane; s < stripes; s += 32) {
