@@ -67,7 +67,7 @@ def pictures():
     meta = {}
     for name, (_, fmt, top, compat) in rp.PICTURES.items():
         cs = rp.stream(name)
-        r = ref_cpu_runner.decode([cs], fmt, threads=4, top_level=top, timeout=300)
+        r = ref_cpu_runner.decode([cs], fmt, threads=1, top_level=top, timeout=300)
         if not r["ok"]:
             raise SystemExit("%s: %s" % (name, r["error"]))
         out = r["outputs"][0]

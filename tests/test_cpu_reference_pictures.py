@@ -139,7 +139,7 @@ def test_oracle_matches_live_reference_on_random_configurations(pkg):
     worst = 0
     for seed in range(700, 724):
         cs, fmt, rev = random_reference_config(seed)
-        r = ref_cpu_runner.decode([cs], fmt, threads=2, timeout=120)
+        r = ref_cpu_runner.decode([cs], fmt, threads=1, timeout=120)  # single-worker engine: its workers race
         assert r["ok"], (seed, r["error"])
         rc, out, _ = oracle_util.oracle_decode(native.Plan(cs), fmt, ref_compat=1 if rev else 0)
         assert rc == 0

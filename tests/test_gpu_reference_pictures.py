@@ -64,7 +64,7 @@ def test_device_matches_reference_picture(gpu_ctx, name):
     assert not g["reversible"], "%s: 5/3 picture differs from the reference's" % name
     if not ref_cpu_runner.available():
         pytest.fail("%s differs from the reference digest and no reference library is here to count LSBs" % name)
-    r = ref_cpu_runner.decode([cs], g["format"], threads=4, top_level=g["top_level"], timeout=300)
+    r = ref_cpu_runner.decode([cs], g["format"], threads=1, top_level=g["top_level"], timeout=300)
     assert r["ok"], r["error"]
     d = compare_with_reference(out, r["outputs"][0], g["format"], False)
     assert d <= NINE_SEVEN_LSB
@@ -104,7 +104,7 @@ def test_device_matches_live_reference_on_random_configurations(gpu_ctx):
     worst = 0
     for seed in range(800, 824):
         cs, fmt, rev = random_reference_config(seed)
-        r = ref_cpu_runner.decode([cs], fmt, threads=4, timeout=120)
+        r = ref_cpu_runner.decode([cs], fmt, threads=1, timeout=120)  # single-worker engine: its workers race
         assert r["ok"], (seed, r["error"])
         out = _device_decode(gpu_ctx, native.Plan(cs), fmt, native.FLAG_REF_COMPAT if rev else 0)
         worst = max(worst, compare_with_reference(out, r["outputs"][0], fmt, rev))
