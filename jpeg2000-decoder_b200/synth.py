@@ -166,7 +166,11 @@ def _cached(key, make):
         d = np.load(path, allow_pickle=False)
         return [bytes(d["s%d" % i]) for i in range(int(d["n"]))]
     streams = make()
-    np.savez(path, n=len(streams), **{"s%d" % i: np.frombuffer(s, np.uint8) for i, s in enumerate(streams)})
+    # several processes (one per GPU) may build the same workload at once: each writes its
+    # own file and renames it into place, so a reader never sees a partly written cache
+    tmp = "%s.%d.tmp.npz" % (path[:-4], os.getpid())
+    np.savez(tmp, n=len(streams), **{"s%d" % i: np.frombuffer(s, np.uint8) for i, s in enumerate(streams)})
+    os.replace(tmp, path)
     return streams
 
 
