@@ -103,6 +103,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+T1_FORMS = {1: "compact (one block per warp)", 2: "unrolled (one block per warp)", 3: "lanes (one block per lane)"}
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -516,7 +519,7 @@ def run_gpu(args, rank, world, dist):
     cfg = dict(cfg)
     cfg.update({"parallelism": "replicas x%d" % world, "l2": "flushed between steps (256 MB write)",
                 "bad_blocks": bad, "cuda_graph": not args.no_graph,
-                "autotuned_t1": ({"form": "compact" if tuned["t1_form"] == 1 else "unrolled",
+                "autotuned_t1": ({"form": T1_FORMS.get(tuned["t1_form"], "auto"),
                                   "warps_per_cta": tuned["t1_warps_per_cta"]} if tuned else None),
                 "autotuned_dwt": ({"coarse_levels": "one shared-memory kernel" if tuned["dwt_coarse"] == 1
                                    else "one launch per level",
@@ -763,7 +766,7 @@ def main():
     ap.add_argument("--decode-repeat", type=int, default=0,
                     help="profiling mode: decode the workload this many times, print stage times, no bench line")
     ap.add_argument("--frames", type=int, default=0, help="profiling mode: only the first N pictures")
-    ap.add_argument("--t1-form", type=int, default=0, help="profiling mode: Tier-1 form 0 auto, 1 compact, 2 unrolled")
+    ap.add_argument("--t1-form", type=int, default=0, help="profiling mode: Tier-1 form 0 auto, 1 compact, 2 unrolled, 3 lanes")
     ap.add_argument("--dwt-coarse", type=int, default=0,
                     help="profiling mode: coarse DWT levels 0 auto, 1 fused into one kernel, 2 one launch per level")
     args = ap.parse_args()

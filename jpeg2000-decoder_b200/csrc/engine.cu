@@ -4,8 +4,9 @@
  * A batch is a set of decode plans.  batch_launch concatenates their Tier-1 work lists,
  * coded bytes and DWT/output task tables into one pinned staging area, copies each
  * section to the device with one cudaMemcpyAsync, then enqueues:
- *   - Tier-1: one persistent launch per code-block size class (<= 32x32, <= 64x64) that
- *     drains a work queue sorted by coded length (longest first);
+ *   - Tier-1: persistent launches that drain work queues sorted by coded length (longest
+ *     first): one code-block per lane (t1_lanes.cuh) for blocks up to 64x64 without bypass
+ *     segments, or one per warp (t1_kernel.cuh) for every block;
  *   - inverse DWT: one launch per level step for all tile-components of all images
  *     (5/3 and 9/7 variants), coarsest level first;
  *   - inverse MCT + DC shift + pack into each image's output;
@@ -31,6 +32,7 @@
 #include "codestream.h"
 #include "dwt_kernel.cuh"
 #include "t1_kernel.cuh"
+#include "t1_lanes.cuh"
 
 using namespace j2k_dev;
 
@@ -58,10 +60,11 @@ struct T1Layout {
   static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 8 + 32) + 15) & ~15;
 };
 
-// Host-side queue classes: code-block size bound.  One class: with 64 registers per thread
-// the register file, not shared memory, limits resident warps, so smaller blocks gain
-// nothing from a smaller per-warp layout, and one launch has one tail instead of two.
-enum { Q64 = 0, NQ = 1 };
+// Host-side queue classes: blocks the lane form decodes (up to 64x64, no bypass segments)
+// and the others; the warp forms take both, as one queue (the two are contiguous).
+enum { QL = 0, QW = 1, NQ = 2 };
+// the lane form's tables follow the warp forms' in the device table buffer
+constexpr size_t LANE_TABLES_OFF = (sizeof(T1Tables) + 255) & ~(size_t)255;
 
 template <int MAXW, int MAXH, bool UNROLLED>
 __device__ __forceinline__ void t1_body(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n,
@@ -356,12 +359,18 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
   for (auto &e : c->ev) cudaEventCreate(&e);
   T1Tables T;
   build_t1_tables(T);
-  if (ensure(c, c->d_tables, sizeof(T1Tables)) != J2K_OK ||
-      cudaMemcpy(c->d_tables.p, &T, sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) {
+  j2k_lanes::LaneTables LT;
+  j2k_lanes::build_lane_tables(LT);
+  if (ensure(c, c->d_tables, LANE_TABLES_OFF + sizeof(LT)) != J2K_OK ||
+      cudaMemcpy(c->d_tables.p, &T, sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy((uint8_t *)c->d_tables.p + LANE_TABLES_OFF, &LT, sizeof(LT), cudaMemcpyHostToDevice) != cudaSuccess) {
     j2k_gpu_ctx_destroy(c);
     return J2K_ERR_CUDA;
   }
   // opt into the large dynamic shared memory of the Tier-1 kernels
+  if (j2k_lanes::CTA_SMEM <= c->smem_optin)
+    cudaFuncSetAttribute(j2k_lanes::t1_kernel_lanes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)j2k_lanes::CTA_SMEM);
   cudaFuncSetAttribute(t1_kernel<64, 64, false>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   cudaFuncSetAttribute(t1_kernel<64, 64, true>(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->smem_optin);
   cudaFuncSetAttribute(last_level_output_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -404,7 +413,7 @@ extern "C" int j2k_gpu_set_tuning(j2k_gpu_ctx *c, const j2k_gpu_tuning *t) {
   if (n.t1_warps_per_cta > 32) n.t1_warps_per_cta = 32;
   if (n.dwt_tile <= 0) n.dwt_tile = 64;
   if (n.dwt_tile != 64) return J2K_ERR_UNSUPPORTED;  // the level kernels are built for 64x64 tiles
-  if (n.t1_form < 0 || n.t1_form > 2) n.t1_form = 0;
+  if (n.t1_form < 0 || n.t1_form > 3) n.t1_form = 0;
   if (n.t1_latency_waves <= 0) n.t1_latency_waves = 2;
   if (n.dwt_coarse < 0 || n.dwt_coarse > 2) n.dwt_coarse = 0;  // takes effect at the next batch_stage
   if (n.use_graph != c->tuning.use_graph || n.t1_form != c->tuning.t1_form || n.dwt_coarse != c->tuning.dwt_coarse ||
@@ -509,30 +518,49 @@ void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, c
                                                                      c->d_A.p, (uint16_t *)c->d_status.p, tab);
 }
 
-// Kernel form: the unrolled (latency) form while the queue holds at most
-// `t1_latency_waves` blocks per resident warp slot of the GPU (the launch's time is then the
-// serial time of its longest blocks), the compact (throughput) form for longer queues.
-template <int MAXW, int MAXH>
-void launch_t1(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
-               const uint32_t *seg, const T1Tables *tab) {
-  bool unrolled;
-  int warps = c->tuning.t1_warps_per_cta;
-  if (c->tuning.t1_form == 1) {
-    unrolled = false;
-  } else if (c->tuning.t1_form == 2) {
-    unrolled = true;
-  } else {
-    auto it = c->tune_table.find(n > 0 ? 31 - __builtin_clz((unsigned)n) : 0);
-    if (it != c->tune_table.end()) {
-      unrolled = it->second.form == 2;
-      warps = it->second.warps;
-    } else {
-      const int waves = c->tuning.t1_latency_waves > 0 ? c->tuning.t1_latency_waves : 2;
-      unrolled = (long long)n <= (long long)waves * c->sm_count * 32;
-    }
+// Tier-1 form for a batch of n code-blocks: 1 compact warp form (throughput), 2 unrolled
+// warp form (latency), 3 one block per lane (throughput), and warps per CTA of a warp form.
+// An explicit tuning.t1_form wins; the auto form (0) takes the autotuned choice of the
+// queue's size bucket, else the unrolled form while the queue holds at most
+// `t1_latency_waves` blocks per resident warp slot of the GPU (the launch's time is then
+// the serial time of its longest blocks) and the lane form for longer queues.
+void t1_shape(const j2k_gpu_ctx *c, int n, int &form, int &warps) {
+  warps = c->tuning.t1_warps_per_cta;
+  if (c->tuning.t1_form >= 1 && c->tuning.t1_form <= 3) {
+    form = c->tuning.t1_form;
+    return;
   }
-  if (unrolled) launch_t1_as<MAXW, MAXH, true>(c, st, n, cbs, ord, cnt, seg, tab, warps);
-  else launch_t1_as<MAXW, MAXH, false>(c, st, n, cbs, ord, cnt, seg, tab, warps);
+  auto it = c->tune_table.find(n > 0 ? 31 - __builtin_clz((unsigned)n) : 0);
+  if (it != c->tune_table.end()) {
+    form = it->second.form;
+    warps = it->second.warps;
+    return;
+  }
+  const int waves = c->tuning.t1_latency_waves > 0 ? c->tuning.t1_latency_waves : 2;
+  form = (long long)n <= (long long)waves * c->sm_count * 32 ? 2 : 3;
+}
+
+// Enqueue the Tier-1 stage: the lane kernel on the lane queue and a warp form on the rest,
+// or a warp form on both queues (contiguous in `ord`).  Returns the number of launches.
+int launch_t1(j2k_gpu_ctx *c, cudaStream_t st, const size_t nq[NQ], const j2k_cblk *cbs, const uint32_t *ord,
+              int *cnt, const uint32_t *seg, const T1Tables *tab, const j2k_lanes::LaneTables *ltab) {
+  const int nl = (int)nq[QL], nw = (int)nq[QW], n = nl + nw;
+  if (!n) return 0;
+  int form, warps;
+  t1_shape(c, n, form, warps);
+  const bool lanes_ok = j2k_lanes::CTA_SMEM <= c->smem_optin;
+  if (form == 3 && nl > 0 && lanes_ok) {
+    const int grid = std::max(1, std::min(c->sm_count, nl));
+    j2k_lanes::t1_kernel_lanes<<<grid, j2k_lanes::CTA_WARPS * 32, j2k_lanes::CTA_SMEM, st>>>(
+        cbs, ord, nl, cnt, (const uint8_t *)c->d_bytes.p, seg, c->d_A.p, (uint16_t *)c->d_status.p, ltab);
+    if (!nw) return 1;
+    launch_t1_as<64, 64, false>(c, st, nw, cbs, ord + nl, cnt + 1, seg, tab, warps);
+    return 2;
+  }
+  if (form == 3) form = 1;  // no lane-form blocks (or too little shared memory): compact warp form
+  if (form == 2) launch_t1_as<64, 64, true>(c, st, n, cbs, ord, cnt, seg, tab, warps);
+  else launch_t1_as<64, 64, false>(c, st, n, cbs, ord, cnt, seg, tab, warps);
+  return 1;
 }
 }  // namespace
 
@@ -576,7 +604,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       cb.out_off += im.coef_base;
       uint32_t idx = (uint32_t)cbs.size();
       cbs.push_back(cb);
-      ordq[Q64].push_back(idx);
+      ordq[j2k_lanes::lane_eligible(cb) ? QL : QW].push_back(idx);
     }
     seg.insert(seg.end(), p.seglens.begin(), p.seglens.end());
     byte_base += p.bytes.size();
@@ -920,15 +948,8 @@ int enqueue_decode(j2k_gpu_ctx *c, cudaStream_t st, bool capturing) {
   const uint32_t *d_seg = (const uint32_t *)(D + o_seg);
   int *cnt = (int *)c->d_counter.p;
   const T1Tables *tab = (const T1Tables *)c->d_tables.p;
-  size_t qoff = 0;
-  for (int q = 0; q < NQ; ++q) {
-    const int n = (int)G.nq[q];
-    if (n) {
-      launch_t1<64, 64>(c, st, n, d_cbs, d_ord + qoff, cnt + q, d_seg, tab);
-      c->launches++;
-    }
-    qoff += G.nq[q];
-  }
+  const auto *ltab = (const j2k_lanes::LaneTables *)((const uint8_t *)c->d_tables.p + LANE_TABLES_OFF);
+  c->launches += launch_t1(c, st, G.nq, d_cbs, d_ord, cnt, d_seg, tab, ltab);
   CK(cudaGetLastError());
   CK(record(c->ev[2], st, capturing));
 
@@ -1213,14 +1234,16 @@ extern "C" int j2k_gpu_autotune(j2k_gpu_ctx *c, void *stream, int iters, j2k_gpu
   if (!c || iters <= 0) return J2K_ERR_ARG;
   if (!c->staged || (c->launched && !c->synced)) return J2K_ERR_STATE;
   const j2k_gpu_tuning saved = c->tuning;
-  const int n = (int)c->sg.nq[Q64];
+  const int n = (int)(c->sg.nq[QL] + c->sg.nq[QW]);
   const int bucket = n > 0 ? 31 - __builtin_clz((unsigned)n) : 0;
   j2k_gpu_ctx::TuneEntry win;
   win.t1_ms = 1e30f;
-  static const int forms[2] = {1, 2};
+  static const int forms[3] = {1, 2, 3};
   static const int widths[3] = {2, 4, 8};
   for (int f : forms)
     for (int w : widths) {
+      // the lane form has one shape (three warps per CTA) and needs lane-form blocks
+      if (f == 3 && (w != 8 || c->sg.nq[QL] == 0 || j2k_lanes::CTA_SMEM > c->smem_optin)) continue;
       j2k_gpu_tuning t = saved;
       t.t1_form = f;
       t.t1_warps_per_cta = w;

@@ -43,9 +43,10 @@ def _decode_check(ctx, cs, fmt, flags=0):
 
 @pytest.mark.parametrize("name", sorted(n for n in os.listdir(GOLDEN) if n.endswith(".j2k")))
 @pytest.mark.parametrize("flags", [0, 1])
-@pytest.mark.parametrize("t1_form", [1, 2])
+@pytest.mark.parametrize("t1_form", [1, 2, 3])
 def test_golden_streams_bit_exact(gpu_ctx, name, flags, t1_form):
-    """Both Tier-1 kernel forms (1 compact, 2 unrolled) on every fixture."""
+    """Every Tier-1 kernel form (1 compact, 2 unrolled, 3 one block per lane, which leaves
+    bypass blocks to the compact form in the same batch) on every fixture."""
     from jpeg2000_decoder_b200 import native
     gpu_ctx.set_tuning(t1_form=t1_form)
     cs = _read(name)
@@ -89,7 +90,7 @@ def test_c1_lossless_and_reference_rows(gpu_ctx):
     assert len(bad) == 31 and bad.min() == 481
 
 
-@pytest.mark.parametrize("t1_form", [1, 2])
+@pytest.mark.parametrize("t1_form", [1, 2, 3])
 def test_c2_97_ict_1bpp_exact_and_fp64_budget(gpu_ctx, t1_form):
     """C2 at full size: 2048x2048 RGB, 9/7 + ICT at ~1 bpp, with both Tier-1 kernel forms."""
     from jpeg2000_decoder_b200 import native, synth
@@ -322,7 +323,7 @@ def test_autotune_and_graph_replay_match_direct_launches(gpu_ctx):
         gpu_ctx.add(p, native.FMT_24BITS_RGB)
     gpu_ctx.stage()
     best, ms = gpu_ctx.autotune(1)
-    assert best["t1_form"] in (1, 2) and best["t1_warps_per_cta"] in (2, 4, 8) and ms > 0
+    assert best["t1_form"] in (1, 2, 3) and best["t1_warps_per_cta"] in (2, 4, 8) and ms > 0
     gpu_ctx.set_tuning(use_graph=1)
     for _ in range(2):
         gpu_ctx.run()
@@ -370,7 +371,7 @@ def test_fused_last_level_equals_kept_components_path(gpu_ctx, name):
 def test_tiny_and_odd_geometries_bit_exact(gpu_ctx, h, w):
     """Pictures smaller than a code-block, one sample wide or high, odd sizes, more DWT
     levels than the size supports: every Tier-1 and DWT edge path, 5/3 and 9/7, one and
-    three components, both Tier-1 kernel forms; GPU equals the oracle (tolerance 0), and
+    three components, every Tier-1 kernel form; GPU equals the oracle (tolerance 0), and
     5/3 equals its source."""
     from jpeg2000_decoder_b200 import native
     rng = np.random.default_rng(h * 1000 + w)
@@ -380,7 +381,7 @@ def test_tiny_and_odd_geometries_bit_exact(gpu_ctx, h, w):
             cs = native.encode(img, 8, reversible=rev, levels=5, cbw_exp=6, cbh_exp=6, num_layers=1,
                                layer_bpp=[0 if rev else 4.0], guard_bits=2 if rev else 1)
             fmt = native.FMT_32BITS_4COMPONENTS if ncomp == 1 else native.FMT_24BITS_RGB
-            for form in (1, 2):
+            for form in (1, 2, 3):
                 gpu_ctx.set_tuning(t1_form=form)
                 out, _ = _decode_check(gpu_ctx, cs, fmt)
                 if rev:
@@ -490,3 +491,45 @@ def test_subsampled_packed_output_needs_full_resolution_first_component(gpu_ctx)
     got = np.empty((32, 32), np.int32)
     assert native.lib().j2k_gpu_component_copy(gpu_ctx.h, slot, 0, got.ctypes.data_as(ctypes.c_void_p), got.nbytes) == 0
     assert np.array_equal(got + 128, img[0][::2, ::2])
+
+
+def test_lane_form_mode_switches_shapes_and_refills(gpu_ctx):
+    """The one-block-per-lane Tier-1 form: context reset, per-pass termination,
+    segmentation symbols, stripe-causal contexts and their combinations, code-block shapes
+    from 4x64 to 64x64, and a batch of more code-blocks than the GPU has lanes (so lanes take
+    second blocks from the queue) holding a bypass picture too (its blocks go to the warp
+    form in the same launch sequence); every Tier-1 coefficient and output pixel equals the
+    oracle's."""
+    from jpeg2000_decoder_b200 import native, synth
+    gpu_ctx.set_tuning(t1_form=3)
+    try:
+        img = synth.fractal_rgb(13, 96, 160, bitdepth=12)
+        for mode in (0x02, 0x04, 0x08, 0x20, 0x2E, 0x10, 0x3E, 0x01):
+            cs = native.encode(img, 12, reversible=1, levels=4, cbw_exp=5, cbh_exp=5, num_layers=3,
+                               layer_bpp=[1, 3, 0], mode=mode)
+            out, _ = _decode_check(gpu_ctx, cs, native.FMT_48BITS_RGB)
+            rgb = out.view(np.uint16).reshape(96, 160, 3)[:, :, ::-1].transpose(2, 0, 1) >> 4
+            assert np.array_equal(rgb, img), mode
+        img8 = synth.fractal_rgb(14, 70, 133)
+        for cw, ch in ((6, 4), (4, 6), (3, 3), (6, 2), (2, 6), (5, 6)):
+            cs = native.encode(img8, 8, reversible=0, levels=3, cbw_exp=cw, cbh_exp=ch, num_layers=2,
+                               layer_bpp=[1, 4], mode=0x08 if cw == 3 else 0)
+            _decode_check(gpu_ctx, cs, native.FMT_24BITS_RGB)
+        # 2 x 3 x 4096 blocks of 8x8: more than 148 SMs x 96 lanes; then a bypass picture
+        big = [native.encode(synth.fields_and_edges(20 + i, 512, 512), 8, reversible=0, levels=5, cbw_exp=3,
+                             cbh_exp=3, num_layers=1, layer_bpp=[2.0]) for i in range(2)]
+        big.append(native.encode(img8, 8, reversible=1, levels=3, mode=0x03))
+        plans = [native.Plan(cs) for cs in big]
+        assert sum(p.info.num_cblks for p in plans) > 148 * 96
+        gpu_ctx.begin()
+        for p in plans:
+            gpu_ctx.add(p, native.FMT_24BITS_RGB)
+        gpu_ctx.launch()
+        assert gpu_ctx.sync() == 0
+        for i, p in enumerate(plans):
+            rc, bad = gpu_ctx.status(i)
+            assert rc == 0 and bad == 0
+            _, want, _ = oracle_util.oracle_decode(p, native.FMT_24BITS_RGB)
+            assert np.array_equal(gpu_ctx.output(i), want), i
+    finally:
+        gpu_ctx.set_tuning()
