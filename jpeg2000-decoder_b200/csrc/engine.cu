@@ -1065,7 +1065,11 @@ extern "C" int j2k_gpu_batch_run(j2k_gpu_ctx *c, void *user_stream) {
   DeviceOrder &order = device_order(c->device);
   std::lock_guard<std::mutex> lk(order.mu);
   if (!order.last) CK(cudaEventCreateWithFlags(&order.last, cudaEventDisableTiming));
-  if (ordered && (long long)c->sg.n_cblks >= (long long)c->sm_count * 32) CK(cudaStreamWaitEvent(st, order.last, 0));
+  int t1_form = 0, t1_warps = 0;
+  t1_shape(c, (int)c->sg.n_cblks, t1_form, t1_warps);
+  const bool fills = (long long)c->sg.n_cblks >= (long long)c->sm_count * 32 ||
+                     (t1_form == 3 && (long long)c->sg.nq[QL] >= c->sm_count);  // a lane-form CTA holds its SM
+  if (ordered && fills) CK(cudaStreamWaitEvent(st, order.last, 0));
   if (c->launched) {
     // a repeated run: no input copies, both copy events at the start
     CK(cudaEventRecord(c->ev[0], st));

@@ -136,6 +136,7 @@ struct Lane {
   uint64_t wmask;     // columns present
   int num_passes, kp, type, p;
   int s, c, wc, k, kind, ctx, flip, run, status;  // wc: the column the windows hold
+  uint32_t e;  // context word of the pending decision, loaded when the decision is set up
   uint32_t rows, vrows;
   uint32_t eL, eC, eR, xL, xC, xR;
   uint32_t pin, rin, dirty;  // pi / rho nibbles of the current column, bits set during the visit
@@ -193,10 +194,10 @@ J2K_LHD void mq_renorm(Lane &m) {
   m.C <<= n;
   m.t -= n;
 }
-// one decision on context slot L.ctx (MQ_DECODE, bmi_mq_decoder.h:86-128)
+// one decision on context slot L.ctx, whose word L.e holds (MQ_DECODE,
+// bmi_mq_decoder.h:86-128)
 J2K_LHD int decide(Lane &L, const LaneMem &M, const LaneTables &T) {
-  uint32_t &slot = M.CX(L.ctx);
-  const uint32_t e = slot;
+  const uint32_t e = L.e;
   const int32_t q = (int32_t)(e & 0x7FFFFFu);
   const int mps = (int)((e >> 23) & 1);
   L.A -= q;
@@ -208,7 +209,7 @@ J2K_LHD int decide(Lane &L, const LaneMem &M, const LaneTables &T) {
   const bool lps = (L.A < q) != ex;
   if (ex) L.A = q;
   else L.C -= q;
-  slot = T.next[e >> 24][lps ? 1 : 0];
+  M.CX(L.ctx) = T.next[e >> 24][lps ? 1 : 0];
   mq_renorm(L);
   return mps ^ (int)lps;
 }
@@ -465,9 +466,8 @@ J2K_LHD void become_significant(Lane &L, const LaneMem &M, int sym) {
   L.base[(size_t)r * L.stride + L.c] = (int32_t)(((uint32_t)sym << 31) + (1u << L.p) + ((1u << L.p) >> 1));
 }
 
-// One MQ decision of a lane with a pending decision, then the next pending decision.
-J2K_LHD void lane_step(Lane &L, const LaneMem &M, const LaneTables &T) {
-  const int d = decide(L, M, T);
+// The outcome `d` of the pending decision; then the next pending decision.
+J2K_LHD void lane_apply(Lane &L, const LaneMem &M, const LaneTables &T, int d) {
   switch (L.kind) {
     case K_ZC:
       if (L.type == P_SP) {
@@ -518,6 +518,13 @@ J2K_LHD void lane_step(Lane &L, const LaneMem &M, const LaneTables &T) {
   next_row(L, M, T);
 }
 
+// One MQ decision of a lane with a pending decision, then the next pending decision and
+// its context word (read now, so the load overlaps the rest of the warp's loop trip).
+J2K_LHD void lane_step(Lane &L, const LaneMem &M, const LaneTables &T) {
+  lane_apply(L, M, T, decide(L, M, T));
+  L.e = M.CX(L.ctx);
+}
+
 // MSB plane and pass count (bmi_block_decoder.cpp:603-622, :708-711)
 J2K_LHD void block_planes(const j2k_cblk &cb, int &bit_plane, int &num_passes) {
   const int missing = cb.missing;
@@ -559,6 +566,7 @@ J2K_LHD void lane_begin(Lane &L, const LaneMem &M, const LaneTables &T, const j2
   L.c = -1;
   L.wc = -2;
   L.k = 0;
+  L.ctx = 0;
   L.pin = L.rin = L.dirty = 0;
   L.eL = L.eC = L.eR = L.xL = L.xC = L.xR = 0;
   block_planes(cb, L.p, L.num_passes);
@@ -571,6 +579,7 @@ J2K_LHD void lane_begin(Lane &L, const LaneMem &M, const LaneTables &T, const j2
     return;
   }
   if (start_pass(L, M)) advance(L, M, T);
+  L.e = M.CX(L.ctx);
 }
 
 // Whether block `cb` is decoded by the lane form: 64x64 at most, no raw (bypass) segments.
