@@ -150,10 +150,11 @@ typedef struct j2k_gpu_tuning {
   int dwt_tile;          /* output tile edge of the DWT level kernels (64; other values are refused) */
   int use_graph;         /* capture Tier-1 + DWT launches of a batch into a CUDA graph */
   int t1_form;           /* Tier-1 kernel form: 0 auto, 1 compact (one block per warp, throughput),
-                            2 unrolled (one block per warp, latency), 3 lanes (one block per lane,
-                            throughput; bypass blocks of the batch go to the compact form) */
+                            2 unrolled (one block per warp, latency), 3 lanes (one block per lane;
+                            bypass blocks of the batch go to the compact form; slower than 1 on
+                            the measured workloads, never chosen by the auto form) */
   int t1_latency_waves;  /* auto form without an autotuned choice: unrolled while code-blocks <=
-                            this many x 32 warps x SMs, lanes above */
+                            this many x 32 warps x SMs, compact above */
   int dwt_coarse;        /* the coarse levels of each tile-component (resolutions up to 64 samples a
                             side) in one shared-memory kernel: 0 default (on), 1 on, 2 off (one
                             launch per level) */
@@ -161,8 +162,7 @@ typedef struct j2k_gpu_tuning {
 int j2k_gpu_set_tuning(j2k_gpu_ctx *ctx, const j2k_gpu_tuning *t);
 int j2k_gpu_get_tuning(const j2k_gpu_ctx *ctx, j2k_gpu_tuning *t);
 /* Autotuner: times the staged batch (`iters` runs after one warm-up run per candidate)
- * under each Tier-1 kernel form (compact and unrolled with CTA widths of 2, 4, 8 warps;
- * the lane form when the batch has blocks it takes) and
+ * under the compact and unrolled Tier-1 kernel forms and CTA widths (2, 4, 8 warps) and
  * records the fastest for batches of this many code-blocks (power-of-two bucket); the
  * auto form (t1_form 0) then uses it for every later batch in that bucket.  Then, with that
  * Tier-1 shape, it times the inverse DWT with the coarse levels fused into one

@@ -4,9 +4,9 @@
  * A batch is a set of decode plans.  batch_launch concatenates their Tier-1 work lists,
  * coded bytes and DWT/output task tables into one pinned staging area, copies each
  * section to the device with one cudaMemcpyAsync, then enqueues:
- *   - Tier-1: persistent launches that drain work queues sorted by coded length (longest
- *     first): one code-block per lane (t1_lanes.cuh) for blocks up to 64x64 without bypass
- *     segments, or one per warp (t1_kernel.cuh) for every block;
+ *   - Tier-1: a persistent launch that drains a work queue sorted by coded length (longest
+ *     first), one code-block per warp (t1_kernel.cuh); on request (t1_form 3) one block per
+ *     lane (t1_lanes.cuh) for blocks up to 64x64 without bypass segments;
  *   - inverse DWT: one launch per level step for all tile-components of all images
  *     (5/3 and 9/7 variants), coarsest level first;
  *   - inverse MCT + DC shift + pack into each image's output;
@@ -519,11 +519,13 @@ void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, c
 }
 
 // Tier-1 form for a batch of n code-blocks: 1 compact warp form (throughput), 2 unrolled
-// warp form (latency), 3 one block per lane (throughput), and warps per CTA of a warp form.
-// An explicit tuning.t1_form wins; the auto form (0) takes the autotuned choice of the
-// queue's size bucket, else the unrolled form while the queue holds at most
-// `t1_latency_waves` blocks per resident warp slot of the GPU (the launch's time is then
-// the serial time of its longest blocks) and the lane form for longer queues.
+// warp form (latency), 3 one block per lane, and warps per CTA of a warp form.  An explicit
+// tuning.t1_form wins; the auto form (0) takes the autotuned choice of the queue's size
+// bucket, else the unrolled form while the queue holds at most `t1_latency_waves` blocks
+// per resident warp slot of the GPU (the launch's time is then the serial time of its
+// longest blocks) and the compact form for longer queues.  The lane form is only taken
+// when asked for: on B200 it measured 4.2x slower than the compact form on 1080p 9/7
+// frames (its lanes' pass walks diverge: 4.4 of 32 threads active per instruction).
 void t1_shape(const j2k_gpu_ctx *c, int n, int &form, int &warps) {
   warps = c->tuning.t1_warps_per_cta;
   if (c->tuning.t1_form >= 1 && c->tuning.t1_form <= 3) {
@@ -537,7 +539,7 @@ void t1_shape(const j2k_gpu_ctx *c, int n, int &form, int &warps) {
     return;
   }
   const int waves = c->tuning.t1_latency_waves > 0 ? c->tuning.t1_latency_waves : 2;
-  form = (long long)n <= (long long)waves * c->sm_count * 32 ? 2 : 3;
+  form = (long long)n <= (long long)waves * c->sm_count * 32 ? 2 : 1;
 }
 
 // Enqueue the Tier-1 stage: the lane kernel on the lane queue and a warp form on the rest,
@@ -1242,12 +1244,10 @@ extern "C" int j2k_gpu_autotune(j2k_gpu_ctx *c, void *stream, int iters, j2k_gpu
   const int bucket = n > 0 ? 31 - __builtin_clz((unsigned)n) : 0;
   j2k_gpu_ctx::TuneEntry win;
   win.t1_ms = 1e30f;
-  static const int forms[3] = {1, 2, 3};
+  static const int forms[2] = {1, 2};
   static const int widths[3] = {2, 4, 8};
   for (int f : forms)
     for (int w : widths) {
-      // the lane form has one shape (three warps per CTA) and needs lane-form blocks
-      if (f == 3 && (w != 8 || c->sg.nq[QL] == 0 || j2k_lanes::CTA_SMEM > c->smem_optin)) continue;
       j2k_gpu_tuning t = saved;
       t.t1_form = f;
       t.t1_warps_per_cta = w;

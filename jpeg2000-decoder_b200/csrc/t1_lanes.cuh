@@ -1,9 +1,14 @@
 /*
- * t1_lanes.cuh — EBCOT Tier-1 with one code-block per lane (throughput form).
+ * t1_lanes.cuh — EBCOT Tier-1 with one code-block per lane (t1_form 3, on request only).
  *
  * The warp-per-block kernels (t1_kernel.cuh) run one serial MQ chain per warp, so 31 of
- * every 32 lanes repeat the same scalar work.  Here every lane decodes its own code-block:
- * one warp instruction advances 32 blocks.  A lane's block state is kept as bit-planes in
+ * every 32 lanes repeat the same scalar work.  Here every lane decodes its own code-block,
+ * so that one warp instruction could advance 32 blocks.  Measured on B200 it does not: on
+ * 16 1080p 9/7 frames it takes 32.0 ms against the compact warp form's 7.6 ms.  The lanes'
+ * pass walks diverge (4.4 of 32 threads active per warp instruction), a decision costs
+ * ~200 thread instructions of state-machine bookkeeping, and the 96 blocks' state fills
+ * shared memory at one warp per scheduler (issue active 18 %).  It stays as an explicit form,
+ * bit-exact, for comparison.  A lane's block state is kept as bit-planes in
  * shared memory, interleaved by lane (element e of lane L at e * 32 + L, so every access
  * of the warp is bank-conflict free whatever position each lane is at):
  *   sig[c], chi[c], pi[c], rho[c]  (c < 64): column bitmaps, bit r = row r of the block:
