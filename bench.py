@@ -467,7 +467,9 @@ def run_gpu(args, rank, world, dist):
     serving = None
     if args.workload != "c5" and not args.no_serving:
         _, spool, _ = workload("c5", False)  # the full pool of 48 distinct seeded requests
-        m = serve_measure(dev, spool, args.serving_requests, args.depth, args.batch_mpix, 0.0, 1, 5 + rank, dist)
+        # two warm-up passes: the device pools and the pinned output buffers reach their
+        # steady-state sizes before the timed pass
+        m = serve_measure(dev, spool, args.serving_requests, args.depth, args.batch_mpix, 0.0, 2, 5 + rank, dist)
         _, serving = serving_summary(m, world)
         serving["stream"] = "C5 mix: %d requests drawn from %d distinct seeded requests" % (
             args.serving_requests, len(spool))
@@ -622,7 +624,7 @@ def serve_measure(dev, pool, n_req, depth, batch_mpix, rate=0.0, warmup=1, seed=
         return time.perf_counter() - t_start, failed[0]
 
     # ---- warm-up: the device pools and pinned buffers grow to their steady-state sizes
-    for _ in range(max(1, warmup)):
+    for _ in range(max(2, warmup)):
         serve_pass(order)
 
     # ---- phase 1: saturation
@@ -761,7 +763,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="skip the Tier-1 shape autotuner")
     ap.add_argument("--no-graph", action="store_true", help="enqueue launches instead of replaying a CUDA graph")
     ap.add_argument("--no-serving", action="store_true", help="skip the shortened serving stream of the default line")
-    ap.add_argument("--serving-requests", type=int, default=480, help="requests of the shortened serving stream")
+    ap.add_argument("--serving-requests", type=int, default=960, help="requests of the shortened serving stream")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 error check")
     ap.add_argument("--decode-repeat", type=int, default=0,
                     help="profiling mode: decode the workload this many times, print stage times, no bench line")
