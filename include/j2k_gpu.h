@@ -152,7 +152,8 @@ typedef struct j2k_gpu_tuning {
   int t1_form;           /* Tier-1 kernel form: 0 auto, 1 compact (one block per warp, throughput),
                             2 unrolled (one block per warp, latency), 3 lanes (one block per lane;
                             bypass blocks of the batch go to the compact form; slower than 1 on
-                            the measured workloads, never chosen by the auto form) */
+                            the measured workloads, never chosen by the auto form; switching to or
+                            from 3 takes effect at the next stage) */
   int t1_latency_waves;  /* auto form without an autotuned choice: unrolled while code-blocks <=
                             this many x 32 warps x SMs, compact above */
   int dwt_coarse;        /* the coarse levels of each tile-component (resolutions up to 64 samples a

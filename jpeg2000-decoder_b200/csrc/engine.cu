@@ -60,8 +60,10 @@ struct T1Layout {
   static constexpr int PER_WARP = ((CWN * 4 + RF_BYTES + N_CTX * 8 + 32) + 15) & ~15;
 };
 
-// Host-side queue classes: blocks the lane form decodes (up to 64x64, no bypass segments)
-// and the others; the warp forms take both, as one queue (the two are contiguous).
+// Host-side queue classes: blocks the lane form decodes (up to 64x64, no bypass segments;
+// filled only when the batch is staged with t1_form 3) and the others; the warp forms take
+// both, as one queue (the two are contiguous), so without the lane form it is one queue
+// sorted longest first.
 enum { QL = 0, QW = 1, NQ = 2 };
 // the lane form's tables follow the warp forms' in the device table buffer
 constexpr size_t LANE_TABLES_OFF = (sizeof(T1Tables) + 255) & ~(size_t)255;
@@ -589,6 +591,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   std::vector<OutTask> ftasks[2];  // fused last levels: [0] 9/7, [1] 5/3
   std::vector<CoarseTask> ctasks[2];  // coarse levels synthesised in shared memory: [0] 9/7, [1] 5/3
   const bool coarse_on = c->tuning.dwt_coarse == 1 || (c->tuning.dwt_coarse == 0 && c->dwt_auto != 2);
+  const bool lane_split = c->tuning.t1_form == 3;  // queue classes for the lane form
   int fwin = 1;
   uint64_t byte_base = 0;
   uint32_t seg_base = 0;
@@ -606,7 +609,7 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
       cb.out_off += im.coef_base;
       uint32_t idx = (uint32_t)cbs.size();
       cbs.push_back(cb);
-      ordq[j2k_lanes::lane_eligible(cb) ? QL : QW].push_back(idx);
+      ordq[lane_split && j2k_lanes::lane_eligible(cb) ? QL : QW].push_back(idx);
     }
     seg.insert(seg.end(), p.seglens.begin(), p.seglens.end());
     byte_base += p.bytes.size();
