@@ -65,22 +65,21 @@ struct T1Layout {
 // both, as one queue (the two are contiguous), so without the lane form it is one queue
 // sorted longest first.
 enum { QL = 0, QW = 1, NQ = 2 };
-// the lane form's tables follow the warp forms' in the device table buffer
-constexpr size_t LANE_TABLES_OFF = (sizeof(T1Tables) + 255) & ~(size_t)255;
+// The warp forms' tables (MQ states, zero-coding / sign contexts, bypass refinement
+// scatter) in constant memory: every lane of a warp reads the same entry, so the constant
+// cache broadcasts it, and the loads need no shared-memory copy per CTA.
+__constant__ T1Tables c_t1tables;
 
 template <int MAXW, int MAXH, bool UNROLLED>
 __device__ __forceinline__ void t1_body(const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n,
                                         int *__restrict__ counter, const uint8_t *__restrict__ bytes,
                                         const uint32_t *__restrict__ seglens, void *__restrict__ coef,
-                                        uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab) {
+                                        uint16_t *__restrict__ status) {
   extern __shared__ __align__(16) uint8_t smem[];
   typedef T1Layout<MAXW, MAXH> Lay;
-  T1Tables &T = *reinterpret_cast<T1Tables *>(smem);
-  for (int i = threadIdx.x; i < (int)(sizeof(T1Tables) / 4); i += blockDim.x)
-    reinterpret_cast<uint32_t *>(smem)[i] = reinterpret_cast<const uint32_t *>(gtab)[i];
-  __syncthreads();
+  const T1Tables &T = c_t1tables;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint8_t *mine = smem + ((sizeof(T1Tables) + 15) & ~15) + warp * Lay::PER_WARP;
+  uint8_t *mine = smem + warp * Lay::PER_WARP;
   BlockSmem b;
   b.cw = reinterpret_cast<uint32_t *>(mine);
   b.rf = mine + Lay::CWN * 4;
@@ -136,14 +135,14 @@ __device__ __forceinline__ void t1_body(const j2k_cblk *__restrict__ cbs, const 
 #define J2K_T1_PARAMS                                                                                   \
   const j2k_cblk *__restrict__ cbs, const uint32_t *__restrict__ order, int n, int *__restrict__ counter, \
       const uint8_t *__restrict__ bytes, const uint32_t *__restrict__ seglens, void *__restrict__ coef,   \
-      uint16_t *__restrict__ status, const T1Tables *__restrict__ gtab
+      uint16_t *__restrict__ status
 template <int MAXW, int MAXH>
 __global__ void __launch_bounds__(256) t1_kernel_compact(J2K_T1_PARAMS) {
-  t1_body<MAXW, MAXH, false>(cbs, order, n, counter, bytes, seglens, coef, status, gtab);
+  t1_body<MAXW, MAXH, false>(cbs, order, n, counter, bytes, seglens, coef, status);
 }
 template <int MAXW, int MAXH>
 __global__ void __launch_bounds__(256, 1) t1_kernel_unrolled(J2K_T1_PARAMS) {
-  t1_body<MAXW, MAXH, true>(cbs, order, n, counter, bytes, seglens, coef, status, gtab);
+  t1_body<MAXW, MAXH, true>(cbs, order, n, counter, bytes, seglens, coef, status);
 }
 #undef J2K_T1_PARAMS
 
@@ -363,9 +362,8 @@ extern "C" int j2k_gpu_ctx_create(int device, size_t mem_budget, j2k_gpu_ctx **o
   build_t1_tables(T);
   j2k_lanes::LaneTables LT;
   j2k_lanes::build_lane_tables(LT);
-  if (ensure(c, c->d_tables, LANE_TABLES_OFF + sizeof(LT)) != J2K_OK ||
-      cudaMemcpy(c->d_tables.p, &T, sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy((uint8_t *)c->d_tables.p + LANE_TABLES_OFF, &LT, sizeof(LT), cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (cudaMemcpyToSymbol(c_t1tables, &T, sizeof(T)) != cudaSuccess || ensure(c, c->d_tables, sizeof(LT)) != J2K_OK ||
+      cudaMemcpy(c->d_tables.p, &LT, sizeof(LT), cudaMemcpyHostToDevice) != cudaSuccess) {
     j2k_gpu_ctx_destroy(c);
     return J2K_ERR_CUDA;
   }
@@ -494,13 +492,12 @@ namespace {
 // shared memory and thread limits from the occupancy calculator), one wave of CTAs.
 template <int MAXW, int MAXH, bool UNROLLED>
 void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, const uint32_t *ord, int *cnt,
-                  const uint32_t *seg, const T1Tables *tab, int warps_per_cta) {
+                  const uint32_t *seg, int warps_per_cta) {
   typedef T1Layout<MAXW, MAXH> Lay;
-  const size_t tsz = (sizeof(T1Tables) + 15) & ~(size_t)15;
   int best_w = 1, best_ctas = 1, best_warps = 0;
   const int wmax = warps_per_cta > 0 ? std::min(8, warps_per_cta) : 8;
   for (int w = 1; w <= wmax; ++w) {
-    const size_t sm = tsz + (size_t)w * Lay::PER_WARP;
+    const size_t sm = (size_t)w * Lay::PER_WARP;
     if (sm > c->smem_optin) break;
     int ctas = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctas, t1_kernel<MAXW, MAXH, UNROLLED>(), w * 32, sm) !=
@@ -514,10 +511,10 @@ void launch_t1_as(j2k_gpu_ctx *c, cudaStream_t st, int n, const j2k_cblk *cbs, c
       best_ctas = ctas;
     }
   }
-  const size_t sm = tsz + (size_t)best_w * Lay::PER_WARP;
+  const size_t sm = (size_t)best_w * Lay::PER_WARP;
   const int grid = std::max(1, std::min((n + best_w - 1) / best_w, c->sm_count * std::max(1, best_ctas)));
   t1_kernel<MAXW, MAXH, UNROLLED>()<<<grid, best_w * 32, sm, st>>>(cbs, ord, n, cnt, (const uint8_t *)c->d_bytes.p, seg,
-                                                                     c->d_A.p, (uint16_t *)c->d_status.p, tab);
+                                                                     c->d_A.p, (uint16_t *)c->d_status.p);
 }
 
 // Tier-1 form for a batch of n code-blocks: 1 compact warp form (throughput), 2 unrolled
@@ -547,7 +544,7 @@ void t1_shape(const j2k_gpu_ctx *c, int n, int &form, int &warps) {
 // Enqueue the Tier-1 stage: the lane kernel on the lane queue and a warp form on the rest,
 // or a warp form on both queues (contiguous in `ord`).  Returns the number of launches.
 int launch_t1(j2k_gpu_ctx *c, cudaStream_t st, const size_t nq[NQ], const j2k_cblk *cbs, const uint32_t *ord,
-              int *cnt, const uint32_t *seg, const T1Tables *tab, const j2k_lanes::LaneTables *ltab) {
+              int *cnt, const uint32_t *seg, const j2k_lanes::LaneTables *ltab) {
   const int nl = (int)nq[QL], nw = (int)nq[QW], n = nl + nw;
   if (!n) return 0;
   int form, warps;
@@ -558,12 +555,12 @@ int launch_t1(j2k_gpu_ctx *c, cudaStream_t st, const size_t nq[NQ], const j2k_cb
     j2k_lanes::t1_kernel_lanes<<<grid, j2k_lanes::CTA_WARPS * 32, j2k_lanes::CTA_SMEM, st>>>(
         cbs, ord, nl, cnt, (const uint8_t *)c->d_bytes.p, seg, c->d_A.p, (uint16_t *)c->d_status.p, ltab);
     if (!nw) return 1;
-    launch_t1_as<64, 64, false>(c, st, nw, cbs, ord + nl, cnt + 1, seg, tab, warps);
+    launch_t1_as<64, 64, false>(c, st, nw, cbs, ord + nl, cnt + 1, seg, warps);
     return 2;
   }
   if (form == 3) form = 1;  // no lane-form blocks (or too little shared memory): compact warp form
-  if (form == 2) launch_t1_as<64, 64, true>(c, st, n, cbs, ord, cnt, seg, tab, warps);
-  else launch_t1_as<64, 64, false>(c, st, n, cbs, ord, cnt, seg, tab, warps);
+  if (form == 2) launch_t1_as<64, 64, true>(c, st, n, cbs, ord, cnt, seg, warps);
+  else launch_t1_as<64, 64, false>(c, st, n, cbs, ord, cnt, seg, warps);
   return 1;
 }
 }  // namespace
@@ -952,9 +949,8 @@ int enqueue_decode(j2k_gpu_ctx *c, cudaStream_t st, bool capturing) {
   const uint32_t *d_ord = (const uint32_t *)(D + o_ord);
   const uint32_t *d_seg = (const uint32_t *)(D + o_seg);
   int *cnt = (int *)c->d_counter.p;
-  const T1Tables *tab = (const T1Tables *)c->d_tables.p;
-  const auto *ltab = (const j2k_lanes::LaneTables *)((const uint8_t *)c->d_tables.p + LANE_TABLES_OFF);
-  c->launches += launch_t1(c, st, G.nq, d_cbs, d_ord, cnt, d_seg, tab, ltab);
+  const auto *ltab = (const j2k_lanes::LaneTables *)c->d_tables.p;
+  c->launches += launch_t1(c, st, G.nq, d_cbs, d_ord, cnt, d_seg, ltab);
   CK(cudaGetLastError());
   CK(record(c->ev[2], st, capturing));
 

@@ -70,7 +70,7 @@ constexpr uint32_t CHI_ALL = (1u << 19) | (1u << 22) | (1u << 25) | (1u << 28);
 
 enum { C_SIG = 0, C_RUN = 9, C_SIGN = 10, C_MAG = 15, C_UNI = 18, N_CTX = 19 };
 
-// Shared tables, filled once per CTA:
+// Read-only tables (constant memory; every lane of a warp reads the same entry):
 //   mq[94]   : entry of state s = idx*2 + mps: .x = Qe << 8 (the scaled register unit),
 //              .y = (mps << 16) | (state after an MPS << 8) | state after an LPS
 //   zc[3][512]: zero-coding context for LL/LH, HL, HH neighbourhoods
