@@ -47,7 +47,7 @@ typedef struct j2k_server_stats {
   double stage_ms;                 /* host time spent assembling and enqueueing batches */
   double enqueue_ms;               /* ... of which in j2k_gpu_batch_launch */
   uint64_t pool_growths;           /* batches that had to enlarge a slot's device pool */
-  uint64_t pinned_allocs;          /* pinned output buffers allocated (not recycled) */
+  uint64_t pinned_allocs;          /* page-locked chunks added to the output arena (>= 256 MB each) */
 } j2k_server_stats;
 
 /* Starts the scheduler thread.  J2K_ERR_NODEVICE without a CUDA device. */

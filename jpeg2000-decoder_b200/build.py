@@ -25,7 +25,8 @@ REF_CPU = os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")
 
 CU_SOURCES = ["engine.cu", "noalloc.cu"]
 CPP_SOURCES = ["codestream.cpp", "plan_api.cpp", "bmi_decoder.cpp", "bmi_jp2dec.cpp", "server.cpp"]
-HEADERS = ["plan.h", "codestream.h", "t1_kernel.cuh", "t1_lanes.cuh", "dwt_kernel.cuh", "bmi_engine.h"]
+HEADERS = ["plan.h", "codestream.h", "t1_kernel.cuh", "t1_lanes.cuh", "dwt_kernel.cuh", "bmi_engine.h",
+           "pinned_arena.h"]
 
 
 def _nvcc():

@@ -253,6 +253,9 @@ struct j2k_gpu_ctx {
   std::vector<BatchImage> imgs;
   uint16_t *h_status = nullptr;  // pinned
   size_t h_status_cap = 0;
+  // outgrown pinned staging / status areas: freeing page-locked memory waits for the whole
+  // device, which would stall other contexts' work in flight, so they go at ctx_destroy
+  std::vector<void *> h_retired;
   bool launched = false, synced = false, staged = false;
   bool copies_pending = false;  // output copies enqueued behind the decode (ev[5] follows them)
   // staged batch (device-resident inputs) for batch_run
@@ -393,6 +396,7 @@ extern "C" void j2k_gpu_ctx_destroy(j2k_gpu_ctx *c) {
     if (b->p) cudaFree(b->p);
   if (c->h_stage) cudaFreeHost(c->h_stage);
   if (c->h_status) cudaFreeHost(c->h_status);
+  for (void *p : c->h_retired) cudaFreeHost(p);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -812,9 +816,9 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   size_t o_byt = align_up(o_ctk + (ctasks[0].size() + ctasks[1].size()) * sizeof(CoarseTask), 256);
   size_t total = align_up(o_byt + S.bytes + 16, 256);
   if (c->h_stage_cap < total) {
-    // grow by half again at least: page-locking is slow and freeing it synchronises
-    const size_t nc = std::max(total, c->h_stage_cap * 3 / 2);
-    if (c->h_stage) cudaFreeHost(c->h_stage);
+    // double at least: page-locking is slow; the outgrown area is kept until ctx_destroy
+    const size_t nc = std::max(total, c->h_stage_cap * 2);
+    if (c->h_stage) c->h_retired.push_back(c->h_stage);
     c->h_stage = nullptr;
     c->h_stage_cap = 0;
     if (cudaMallocHost(&c->h_stage, nc) != cudaSuccess) {
@@ -903,8 +907,8 @@ extern "C" int j2k_gpu_batch_stage(j2k_gpu_ctx *c, void *user_stream) {
   c->sg.maxL = maxL;
   c->sg.dtask_off = dtask_off;
   if (c->h_status_cap < S.cblks + 1) {
-    const size_t nc = std::max(S.cblks + 1, c->h_status_cap * 3 / 2);
-    if (c->h_status) cudaFreeHost(c->h_status);
+    const size_t nc = std::max(S.cblks + 1, c->h_status_cap * 2);
+    if (c->h_status) c->h_retired.push_back(c->h_status);
     c->h_status = nullptr;
     c->h_status_cap = 0;
     if (cudaMallocHost(&c->h_status, nc * 2) != cudaSuccess) {

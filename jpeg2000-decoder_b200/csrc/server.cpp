@@ -16,6 +16,7 @@
 // another; the engine starts a batch whose Tier-1 fills the GPU only after the previous
 // decode, see j2k_gpu_batch_run).
 #include "../../include/j2k_server.h"
+#include "pinned_arena.h"
 
 #include <cuda_runtime.h>
 
@@ -49,40 +50,18 @@ struct Request {
   Clock::time_point t_submit, t_done;
 };
 
-// Pinned host buffers for decoded pictures, recycled between requests (page-locking is far
-// slower than a copy, so buffers are kept rather than freed)
-struct PinnedPool {
-  std::mutex mu;
-  std::multimap<size_t, uint8_t *> free_bufs;
-  std::map<uint8_t *, size_t> caps;
-  uint8_t *get(size_t n, bool *fresh) {
-    *fresh = false;
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      auto it = free_bufs.lower_bound(n);
-      if (it != free_bufs.end() && it->first <= 2 * n + (1 << 20)) {
-        uint8_t *p = it->second;
-        free_bufs.erase(it);
-        return p;
-      }
-    }
-    const size_t cap = (n + (1 << 20) - 1) & ~(size_t)((1 << 20) - 1);
-    uint8_t *p = nullptr;
-    if (cudaMallocHost((void **)&p, cap) != cudaSuccess) return nullptr;
-    *fresh = true;
-    std::lock_guard<std::mutex> lk(mu);
-    caps[p] = cap;
-    return p;
+// Pinned host memory for decoded pictures: pieces of page-locked chunks, recycled between
+// requests of any size (pinned_arena.h)
+void *page_locked_alloc(size_t n) {
+  void *p = nullptr;
+  if (cudaMallocHost(&p, n) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
   }
-  void put(uint8_t *p) {
-    if (!p) return;
-    std::lock_guard<std::mutex> lk(mu);
-    free_bufs.insert({caps[p], p});
-  }
-  ~PinnedPool() {
-    for (auto &kv : caps) cudaFreeHost(kv.first);
-  }
-};
+  return p;
+}
+void page_locked_free(void *p) { cudaFreeHost(p); }
+typedef j2k::PinnedArena<void *(*)(size_t), void (*)(void *)> PinnedPool;
 
 struct Slot {
   j2k_gpu_ctx *ctx = nullptr;
@@ -107,7 +86,7 @@ struct j2k_server {
   j2k_server_config cfg{};
   size_t slot_budget = 0;
   std::vector<Slot> slots;
-  PinnedPool pinned;
+  PinnedPool pinned{page_locked_alloc, page_locked_free};
   std::mutex mu;
   std::condition_variable cv_submit, cv_done;
   std::deque<Request *> pending;
