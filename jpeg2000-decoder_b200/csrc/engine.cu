@@ -307,7 +307,11 @@ int cuda_fail(cudaError_t e) {
 int ensure(j2k_gpu_ctx *c, DevBuf &b, size_t need) {
   if (need == 0) need = 16;
   if (b.cap >= need) return J2K_OK;
-  size_t nc = std::max(need, b.cap + b.cap / 2);
+  // grow to twice the old size at least (within the budget): replacing a device buffer
+  // frees the old one, which waits for the whole device, and allocating gigabytes takes
+  // hundreds of milliseconds, so a pool warmed on a stream of mixed batches should not have
+  // to grow again for a batch a little larger than the ones it has seen
+  size_t nc = std::max(need, b.cap * 2);
   if (c->reserved - b.cap + nc > c->budget) {
     nc = need;
     if (c->reserved - b.cap + nc > c->budget) return J2K_ERR_NOMEM;
