@@ -469,9 +469,9 @@ def run_gpu(args, rank, world, dist):
     serving = None
     if args.workload != "c5" and not args.no_serving:
         _, spool, _ = workload("c5", False)  # the full pool of 48 distinct seeded requests
-        # two warm-up passes: the device pools and the pinned output buffers reach their
+        # three warm-up passes: the device pools and the pinned output arena reach their
         # steady-state sizes before the timed pass
-        m = serve_measure(dev, spool, args.serving_requests, args.depth, args.batch_mpix, 0.0, 2, 5 + rank, dist)
+        m = serve_measure(dev, spool, args.serving_requests, args.depth, args.batch_mpix, 0.0, 3, 5 + rank, dist)
         _, serving = serving_summary(m, world)
         serving["stream"] = "C5 mix: %d requests drawn from %d distinct seeded requests" % (
             args.serving_requests, len(spool))
@@ -628,7 +628,7 @@ def serve_measure(dev, pool, n_req, depth, batch_mpix, rate=0.0, warmup=1, seed=
         return time.perf_counter() - t_start, failed[0]
 
     # ---- warm-up: the device pools and pinned buffers grow to their steady-state sizes
-    for _ in range(max(2, warmup)):
+    for _ in range(max(3, warmup)):
         serve_pass(order)
 
     # ---- phase 1: saturation
