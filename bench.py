@@ -340,10 +340,22 @@ def fp64_check(ctx, plans, fmt, frames=2, fmts=None):
             "against": "FP64 T.800 dequantisation + 9/7 synthesis + ICT of the same Tier-1 values, before rounding"}
 
 
+def build_workloads_once(items, rank, dist):
+    """Rank 0 encodes the workloads ((name, quick) pairs) into the cache while the other
+    ranks wait, so N ranks do not all encode the same pictures at once."""
+    if dist:
+        if rank == 0:
+            for name, quick in items:
+                workload(name, quick)
+        dist.barrier()
+
+
 def run_gpu(args, rank, world, dist):
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
+    build_workloads_once([(args.workload, args.quick)] +
+                         ([("c5", False)] if args.workload != "c5" and not args.no_serving else []), rank, dist)
     cfg, streams, fmt = workload(args.workload, args.quick)
     pool = ThreadPoolExecutor(max_workers=os.cpu_count())
     plans = parse_all(streams, pool)
@@ -684,6 +696,7 @@ def run_serve(args, rank, world, dist):
     import torch
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
+    build_workloads_once([("c5", args.quick)], rank, dist)
     cfg, pool, _ = workload("c5", args.quick)
     n_req = args.requests or (200 if args.quick else 2000)
     clk = ClockSampler(dev)
