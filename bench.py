@@ -475,7 +475,10 @@ def run_gpu(args, rank, world, dist):
     ctx2.close()
 
     # ---- PSNR / max-abs of the FP32 9/7 path against an FP64 synthesis of the same Tier-1
-    fp64 = fp64_check(ctx, plans, fmt) if not plans[0].info.reversible and not args.no_fp64 else None
+    # (rank 0 only: it is reported once, and the FP64 synthesis is host work the other ranks'
+    # processes would repeat on the same cores)
+    fp64 = (fp64_check(ctx, plans, fmt) if rank == 0 and not plans[0].info.reversible and not args.no_fp64
+            else None)
 
     # ---- a shortened serving stream (C5 mix) through the continuous-batching service
     serving = None
